@@ -1,0 +1,347 @@
+"""Benchmark: GW self-energy builds per second on B200 (one HF-exchange / GW iteration path).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config cfg2|cfg1] [--precision split|fp64]
+
+One step = one full GW Sigma build (G unfold, P0, IR transforms, FP64 Dyson, Sigma) of the
+configured system with V, G and the IR transforms already resident in HBM.  The default
+workload is the 4x4x4 k-mesh, nao = 52, NQ = 400, 72 tau / 69 bosonic frequencies system
+(full BZ, identity symmetry) with seeded synthetic G and V; V (36 GB) is larger than L2.
+
+Prints one JSON line (rank 0).  For N > 1 (torchrun), the irreducible q points are
+distributed round-robin over ranks and the partial Sigma are summed with an NCCL
+all-reduce, as the reference distributes q over device ranks and all-reduces Sigma.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "cfg1": dict(mesh=(2, 2, 2), nao=26, NQ=120),
+    "cfg2": dict(mesh=(4, 4, 4), nao=52, NQ=400),
+}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = str(device_index)
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.dev, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, nm in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def make_inputs(cfg, device, seed=0):
+    """Seeded synthetic system; V generated directly in HBM (36 GB for cfg2)."""
+    import torch
+    from green_gpu_b200 import synth
+    s = synth.make_system(seed=seed, with_V=False, **CONFIGS[cfg])
+    npairs = int(s.irre_pos_kpair.max()) + 1
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    V = torch.empty((npairs, s.NQ, s.nao, s.nao, 2), dtype=torch.float64, device=device)
+    chunk = max(1, npairs // 16)
+    scale = torch.exp(-0.1 * torch.arange(s.NQ, device=device, dtype=torch.float64)).view(1, s.NQ, 1, 1, 1)
+    for p0 in range(0, npairs, chunk):
+        blk = V[p0:p0 + chunk]
+        blk.normal_(generator=g)
+        blk.mul_(scale / np.sqrt(2.0))
+    # V(k,k) must be Hermitian in (i, j): symmetrise the diagonal k-pairs on the device
+    for k in range(s.nk):
+        p = int(s.irre_pos_kpair[k * (k + 1) // 2 + k])
+        Vc = torch.view_as_complex(V[p])
+        Vc.copy_(0.5 * (Vc + Vc.conj().transpose(-1, -2)))
+    torch.cuda.synchronize(device)
+    return s, V
+
+
+def oracle_cpu_baseline(cfg, budget_s=20.0):
+    """Time the FP64 oracle on a bounded sample of the workload and extrapolate to builds/s.
+
+    Sample: P0 of one q over a few k, Sigma of a few (k, q') pairs, Dyson + IR of one q;
+    a build is nq*nk P0 pairs + nq (IR + Dyson) + ink*nq Sigma pairs.
+    """
+    import oracle.gw as ogw
+    from green_gpu_b200 import synth
+    s = synth.make_system(seed=1, **CONFIGS[cfg]) if cfg == "cfg1" else None
+    if s is None:
+        # cfg2-shaped sample with a 2-pair store (the per-pair cost does not depend on nk)
+        s = synth.make_system(mesh=(2, 1, 1), nao=CONFIGS[cfg]["nao"], NQ=CONFIGS[cfg]["NQ"], seed=1)
+    nts, nk = s.nts, s.nk
+    Gf = ogw.g_full(s)
+    tt = np.arange(nts // 2)
+    pref = -2.0
+    t0 = time.perf_counter()
+    n_p0 = 0
+    from oracle.symmetry import coulomb
+    while time.perf_counter() - t0 < budget_s * 0.4 or n_p0 == 0:
+        k = n_p0 % nk
+        k1 = int(s.k1_from_k2q[k * s.nq + 0])
+        V = coulomb(s, k, k1)
+        ogw.p0_pair(V, Gf[k1, 0, tt], Gf[k, 0, nts - 1 - tt], pref)
+        n_p0 += 1
+    t_p0 = (time.perf_counter() - t0) / n_p0
+    t0 = time.perf_counter()
+    P0 = np.zeros((nts, s.NQ, s.NQ), np.complex128)
+    for t in range(nts):
+        X = np.random.default_rng(t).standard_normal((s.NQ, s.NQ)) * 1e-3
+        P0[t] = -(X @ X.T)
+    Pw = ogw.transform_tw(P0, s.Tnt_BF)
+    Ww = ogw.dyson(Pw, "cholesky")
+    Wt = ogw.transform_wt(Ww, s.Ttn_FB)
+    t_q = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    n_sg = 0
+    while time.perf_counter() - t0 < budget_s * 0.4 or n_sg == 0:
+        k1 = int(s.k2_from_k1q[0 * s.nq + (n_sg % nk)])
+        V = coulomb(s, 0, k1)
+        ogw.sigma_pair(V, Gf[k1, 0], Wt)
+        n_sg += 1
+    t_sg = (time.perf_counter() - t0) / n_sg
+    NK = int(np.prod(CONFIGS[cfg]["mesh"]))
+    t_build = NK * NK * t_p0 + NK * t_q + NK * NK * t_sg
+    cores = os.cpu_count()
+    return {"value": 1.0 / t_build, "unit": "builds/s", "cores": cores, "kind": "port",
+            "sample": f"numpy FP64 oracle, {cfg}: {n_p0} P0 (q,k) pairs, 1 q of IR+Dyson, {n_sg} Sigma (k,q') "
+                      f"pairs timed; per-pair times x {NK}x{NK} pairs + {NK} q; OpenBLAS threads = all cores",
+            "seconds_per_build": t_build}
+
+
+def run_reference(args):
+    """Reference arm: the reference's CPU path is the oracle port here (the reference itself
+    cannot be built: MPI, HDF5, Eigen and the green-* repositories are absent)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    steps = []
+    cb = None
+    for _ in range(args.warmup + args.steps):
+        cb = oracle_cpu_baseline(args.config, budget_s=4.0)
+        steps.append(cb["seconds_per_build"])
+    timed = steps[args.warmup:]
+    v = len(timed) / sum(timed)
+    line = {"metric": "GW Sigma builds/s", "value": v, "unit": "builds/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(timed) / len(timed),
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"GW Sigma build, {args.config}", **{k: str(v_) for k, v_ in CONFIGS[args.config].items()}},
+            "cpu_baseline": {**{k: cb[k] for k in ("unit", "cores", "kind", "sample")}, "value": v},
+            "e2e": {"value": v, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cfg2", choices=sorted(CONFIGS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
+    ap.add_argument("--solver", default="cholesky", choices=["cholesky", "lu"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    from green_gpu_b200 import native
+    from green_gpu_b200.synth import gw_flop_model, gw_flop_parts
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(minutes=10), device_id=dev)
+
+    s, V = make_inputs(args.config, dev)
+    ctx = native.Context(s.nk, s.ink, s.inq, s.nao, s.NQ, s.ns, s.nts, s.nw_b, device=local)
+    ctx.set_symmetry(s.k_full_to_reduced, s.k_reduced_to_full, s.k_tr_conj, s.q_full_to_reduced,
+                     s.q_reduced_to_full, s.q_tr_conj, s.k1_from_k2q, s.k2_from_k1q)
+    ctx.set_kpairs(int(s.irre_pos_kpair.max()) + 1, s.conj_kpair_list, s.trans_kpair_list, s.irre_pos_kpair)
+    ctx.set_coulomb_device(V.data_ptr(), V)
+    ctx.set_ir(s.Ttn_FB, s.Tnt_BF)
+    ctx.set_q_shard(rank, world)
+    prec = native.PREC_SPLIT if args.precision == "split" else native.PREC_FP64
+    solver = native.SOLVER_CHOLESKY if args.solver == "cholesky" else native.SOLVER_LU
+    G_host = torch.from_numpy(s.G_tskij.view(np.float64)).pin_memory()
+    G = G_host.to(dev)
+    Sigma = torch.empty_like(G)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        ctx.gw_sigma_device(G.data_ptr(), Sigma.data_ptr(), solver=solver, precision=prec,
+                            stream=stream.cuda_stream)
+        if world > 1:
+            dist.all_reduce(Sigma)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    ctx.set_profiling(True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    lat = []
+    launches = 0
+    kstats = {0: [0, 0.0, 0.0], 1: [0, 0.0, 0.0]}
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step()
+            b.record(stream)
+            b.synchronize()
+            lat.append(a.elapsed_time(b) * 1e-3)
+            launches += ctx.launch_count()
+            for w in (0, 1):
+                st = ctx.kernel_stats(w)
+                kstats[w][0] += st["launches"]
+                kstats[w][1] += st["seconds"]
+                kstats[w][2] += st["flops"]
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    ctx.set_profiling(False)
+    elapsed = e0.elapsed_time(e1) * 1e-3
+    if world > 1:
+        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    value = args.steps / elapsed
+
+    # end to end through the host-buffer C ABI call (H2D of G from pinned memory, D2H of Sigma)
+    e2e_vals = []
+    out_host = np.empty_like(s.G_tskij)
+    G_pinned_np = G_host.numpy().view(np.complex128).reshape(s.G_tskij.shape)
+    for _ in range(max(1, min(2, args.steps))):
+        ctx.gw_sigma(G_pinned_np, solver=solver, precision=prec) if world == 1 else step()
+        e2e_vals.append(ctx.timings().get("e2e", 0.0) if world == 1 else None)
+    e2e_t = [x for x in e2e_vals if x]
+    gbytes = s.G_tskij.nbytes
+
+    # roofline of the dominant contraction (largest device time)
+    pk, pk_src = peaks()
+    dom = max((0, 1), key=lambda w: kstats[w][1])
+    n_l, sec, fl = kstats[dom]
+    achieved = fl / sec / 1e12 if sec > 0 else 0.0
+    fp64_peak = float(os.environ.get("GG_FP64_PEAK_TFLOPS", "40.0"))
+    if args.precision == "fp64":
+        peak, peak_note = fp64_peak, "nominal FP64 tensor (DMMA) peak of B200; no measured FP64 figure"
+    else:
+        peak, peak_note = 2.0 * pk["bf16_tflops"], f"2x {pk_src} bf16 (dense INT8 rate)"
+    roof = {"bound": "tensor", "kernel": "p0_contraction" if dom == 0 else "sigma_contraction",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+            "traffic": None, "launches": n_l, "avg_launch_ms": 1e3 * sec / max(n_l, 1), "peak_source": peak_note}
+    traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(traffic_file):
+        with open(traffic_file) as f:
+            tr = json.load(f).get(f"{roof['kernel']}_{args.precision}_{args.config}")
+        if tr:
+            roof["traffic"] = tr
+
+    flops_build = gw_flop_model(s.nk, s.ink, s.inq, s.ns, s.nts, s.nw_b, s.nao, s.NQ)
+    line = {
+        "metric": "GW Sigma builds/s", "value": value, "unit": "builds/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic (seeded G from random Hermitian Fock, Gaussian V*exp(-0.1Q))",
+        "config": {"workload": f"GW Sigma build {args.config}", "mesh": "x".join(map(str, CONFIGS[args.config]["mesh"])),
+                   "nao": s.nao, "NQ": s.NQ, "nts": s.nts, "nw_b": s.nw_b, "precision": args.precision,
+                   "solver": args.solver, "l2": "inputs larger than L2 (V = %.1f GB)" % (V.numel() * 8 / 1e9),
+                   "parallelism": f"q-shard x{world}" if world > 1 else "1 GPU"},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "model_tflops": flops_build * value / 1e12,
+        "phases_s": ctx.timings(),
+        "roofline": roof,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "e2e": {"value": (1.0 / statistics.mean(e2e_t)) if e2e_t else None, "unit": "builds/s",
+                "h2d_bytes_per_step": gbytes, "d2h_bytes_per_step": gbytes},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = oracle_cpu_baseline(args.config)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

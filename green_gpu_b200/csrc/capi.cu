@@ -1,0 +1,363 @@
+// extern "C" entry points of libgreen_b200.so (declared in include/green_b200.h).
+// No C++ exception crosses this boundary: every call returns a GG_* status and keeps
+// the message for gg_last_error().
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "context.cuh"
+#include "engine.cuh"
+#include "kernels.cuh"
+
+using namespace gg;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+template <typename F>
+int guarded(gg_context* c, F&& f) {
+  if (!c) return GG_ERR_ARG;
+  try {
+    GG_CUDA(cudaSetDevice(c->device));
+    f();
+    c->err.clear();
+    return GG_OK;
+  } catch (const Error& e) {
+    c->err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    c->err = e.what();
+    return GG_ERR_INTERNAL;
+  } catch (...) {
+    c->err = "unknown error";
+    return GG_ERR_INTERNAL;
+  }
+}
+
+void check_shape(const gg_shape& s) {
+  auto bad = [](const std::string& m) { throw Error(GG_ERR_ARG, "shape: " + m); };
+  if (s.nk <= 0 || s.ink <= 0 || s.ink > s.nk) bad("need 0 < ink <= nk");
+  if (s.nq != s.nk) bad("nq must equal nk");
+  if (s.inq <= 0 || s.inq > s.nq) bad("need 0 < inq <= nq");
+  if (s.nao <= 0 || s.NQ <= 0) bad("nao and NQ must be positive");
+  if (s.ns != 1 && s.ns != 2) bad("ns must be 1 or 2");
+  if (s.nts < 4 || s.nts % 2) bad("nts must be even and >= 4 (gw_gpu_kernel.h:67)");
+  if (s.nw_b < 0 || s.nw_b > s.nts) bad("need 0 <= nw_b <= nts (cugw_qpt.cu:79; 0 for HF-only contexts)");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gg_version(void) { return "green-b200 0.1 (sm_100a; FP64 DMMA engine)"; }
+
+int gg_create(const gg_shape* shape, int device, gg_context** out) {
+  if (!shape || !out) return GG_ERR_ARG;
+  *out = nullptr;
+  gg_context* c = nullptr;
+  try {
+    check_shape(*shape);
+    int ndev = 0;
+    GG_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) throw Error(GG_ERR_ARG, "no CUDA device " + std::to_string(device));
+    GG_CUDA(cudaSetDevice(device));
+    c = new gg_context();
+    c->sh = *shape;
+    c->device = device;
+    GG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    *out = c;
+    g_create_error.clear();
+    return GG_OK;
+  } catch (const Error& e) {
+    g_create_error = e.what();
+    delete c;
+    return e.code;
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    delete c;
+    return GG_ERR_INTERNAL;
+  }
+}
+
+void gg_destroy(gg_context* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  delete c;
+}
+
+const char* gg_last_error(const gg_context* c) { return c ? c->err.c_str() : g_create_error.c_str(); }
+
+int gg_set_symmetry(gg_context* c, const int64_t* k_f2r, const int64_t* k_r2f, const int64_t* k_tr,
+                    const int64_t* q_f2r, const int64_t* q_r2f, const int64_t* q_tr, const int64_t* k1q,
+                    const int64_t* k2q, const double* U_k, const double* U_q) {
+  return guarded(c, [&] {
+    if (!k_f2r || !k_r2f || !k_tr || !q_f2r || !q_r2f || !q_tr || !k1q || !k2q)
+      throw Error(GG_ERR_ARG, "symmetry: index arrays must not be NULL");
+    const auto& s = c->sh;
+    auto range = [](const int64_t* a, long n, long hi, const char* what) {
+      for (long i = 0; i < n; ++i)
+        if (a[i] < 0 || a[i] >= hi) throw Error(GG_ERR_ARG, std::string("symmetry: ") + what + " out of range");
+    };
+    range(k_f2r, s.nk, s.ink, "k_full_to_reduced");
+    range(k_r2f, s.ink, s.nk, "k_reduced_to_full");
+    range(q_f2r, s.nq, s.inq, "q_full_to_reduced");
+    range(q_r2f, s.inq, s.nq, "q_reduced_to_full");
+    range(k1q, (long)s.nk * s.nq, s.nk, "k1_from_k2q");
+    range(k2q, (long)s.nk * s.nq, s.nk, "k2_from_k1q");
+    for (long i = 0; i < s.ink; ++i)
+      if (k_f2r[k_r2f[i]] != i) throw Error(GG_ERR_ARG, "symmetry: k maps are inconsistent");
+    for (long i = 0; i < s.inq; ++i)
+      if (q_f2r[q_r2f[i]] != i) throw Error(GG_ERR_ARG, "symmetry: q maps are inconsistent");
+    c->k_f2r.assign(k_f2r, k_f2r + s.nk);
+    c->k_r2f.assign(k_r2f, k_r2f + s.ink);
+    c->k_tr.assign(k_tr, k_tr + s.nk);
+    c->q_f2r.assign(q_f2r, q_f2r + s.nq);
+    c->q_r2f.assign(q_r2f, q_r2f + s.inq);
+    c->q_tr.assign(q_tr, q_tr + s.nq);
+    c->k1_from_k2q.assign(k1q, k1q + (size_t)s.nk * s.nq);
+    c->k2_from_k1q.assign(k2q, k2q + (size_t)s.nk * s.nq);
+    c->k_stars.assign(s.ink, {});
+    c->q_stars.assign(s.inq, {});
+    for (int k = 0; k < s.nk; ++k) c->k_stars[k_f2r[k]].push_back(k);
+    for (int q = 0; q < s.nq; ++q) c->q_stars[q_f2r[q]].push_back(q);
+    std::vector<int> f2r(s.nk), tr(s.nk);
+    for (int k = 0; k < s.nk; ++k) {
+      f2r[k] = (int)k_f2r[k];
+      tr[k] = k_tr[k] != 0;
+    }
+    c->k_f2r_d.upload(f2r.data(), f2r.size(), c->stream);
+    c->k_tr_d.upload(tr.data(), tr.size(), c->stream);
+    const long nn = (long)s.nao * s.nao, NN = (long)s.NQ * s.NQ;
+    c->has_Uk = U_k != nullptr;
+    c->has_Uq = U_q != nullptr;
+    if (U_k) c->Uk.upload((const double2*)U_k, (size_t)s.nk * nn, c->stream);
+    if (U_q) c->Uq.upload((const double2*)U_q, (size_t)s.nq * NN, c->stream);
+    GG_CUDA(cudaStreamSynchronize(c->stream));
+    c->has_sym = true;
+  });
+}
+
+int gg_set_kpairs(gg_context* c, int64_t nstored, const int64_t* conj_list, const int64_t* trans_list,
+                  const int64_t* irre_pos) {
+  return guarded(c, [&] {
+    if (!conj_list || !trans_list || !irre_pos || nstored <= 0) throw Error(GG_ERR_ARG, "kpairs: bad arguments");
+    const long npairs = (long)c->sh.nk * (c->sh.nk + 1) / 2;
+    for (long i = 0; i < npairs; ++i) {
+      if (conj_list[i] < 0 || conj_list[i] >= npairs || trans_list[i] < 0 || trans_list[i] >= npairs ||
+          irre_pos[i] < -1 || irre_pos[i] >= nstored)
+        throw Error(GG_ERR_ARG, "kpairs: entry " + std::to_string(i) + " out of range");
+    }
+    c->nstored = nstored;
+    c->conj_list.assign(conj_list, conj_list + npairs);
+    c->trans_list.assign(trans_list, trans_list + npairs);
+    c->irre_pos.assign(irre_pos, irre_pos + npairs);
+    c->has_kpairs = true;
+  });
+}
+
+int gg_set_coulomb(gg_context* c, const double* V) {
+  return guarded(c, [&] {
+    if (!V) throw Error(GG_ERR_ARG, "coulomb: NULL");
+    if (!c->has_kpairs) throw Error(GG_ERR_STATE, "coulomb: call gg_set_kpairs first");
+    const size_t count = (size_t)c->nstored * c->sh.NQ * c->sh.nao * c->sh.nao;
+    c->V_owned.upload((const double2*)V, count, c->stream);
+    GG_CUDA(cudaStreamSynchronize(c->stream));
+    c->V = c->V_owned.p;
+  });
+}
+
+int gg_set_coulomb_device(gg_context* c, const void* V) {
+  return guarded(c, [&] {
+    if (!V) throw Error(GG_ERR_ARG, "coulomb: NULL");
+    if ((reinterpret_cast<uintptr_t>(V) & 15) != 0) throw Error(GG_ERR_ARG, "coulomb: device pointer not 16-byte aligned");
+    if (!c->has_kpairs) throw Error(GG_ERR_STATE, "coulomb: call gg_set_kpairs first");
+    cudaPointerAttributes attr{};
+    GG_CUDA(cudaPointerGetAttributes(&attr, V));
+    if (attr.type != cudaMemoryTypeDevice || attr.device != c->device)
+      throw Error(GG_ERR_ARG, "coulomb: pointer is not device memory of this context's device");
+    c->V_owned.release();
+    c->V = (const double2*)V;
+  });
+}
+
+int gg_set_ir(gg_context* c, const double* Ttn_FB, const double* Tnt_BF) {
+  return guarded(c, [&] {
+    if (!Ttn_FB || !Tnt_BF) throw Error(GG_ERR_ARG, "ir: NULL");
+    if (c->sh.nw_b <= 0) throw Error(GG_ERR_ARG, "ir: the context was created with nw_b = 0");
+    const int T = c->sh.nts, T2 = T / 2, nw = c->sh.nw_b;
+    c->Ttn.upload((const double2*)Ttn_FB, (size_t)T * nw, c->stream);
+    // Tnt_BF acts on tau points 1..T-2; P0(tau_{T-1-t}) = P0(tau_t) lets the columns of the
+    // mirrored half be added onto their partners: fold[w][t-1] = Tnt[w][t-1] + Tnt[w][T-2-t]
+    // for t = 1..T/2-1 (t = T-1-t never happens for even T).
+    const double2* Tn = (const double2*)Tnt_BF;
+    std::vector<double2> fold((size_t)nw * (T2 - 1));
+    for (int w = 0; w < nw; ++w)
+      for (int t = 1; t < T2; ++t) {
+        double2 a = Tn[(size_t)w * (T - 2) + (t - 1)];
+        double2 b = Tn[(size_t)w * (T - 2) + (T - 2 - t)];
+        fold[(size_t)w * (T2 - 1) + (t - 1)] = make_double2(a.x + b.x, a.y + b.y);
+      }
+    c->Tnt_fold.upload(fold.data(), fold.size(), c->stream);
+    GG_CUDA(cudaStreamSynchronize(c->stream));
+    c->has_ir = true;
+  });
+}
+
+int gg_set_q_shard(gg_context* c, int rank, int size) {
+  return guarded(c, [&] {
+    if (size < 1 || rank < 0 || rank >= size) throw Error(GG_ERR_ARG, "q shard: need 0 <= rank < size");
+    c->shard_rank = rank;
+    c->shard_size = size;
+  });
+}
+
+int gg_set_split_slices(gg_context* c, int slices) {
+  return guarded(c, [&] {
+    if (slices < 2 || slices > 8) throw Error(GG_ERR_ARG, "split slices must be in [2, 8]");
+    c->slices = slices;
+  });
+}
+
+int gg_set_capture(gg_context* c, double* P0_out, double* Pw_out, double* Wt_out) {
+  return guarded(c, [&] {
+    c->cap_P0 = P0_out;
+    c->cap_Pw = Pw_out;
+    c->cap_Wt = Wt_out;
+  });
+}
+
+int gg_gw_sigma_device(gg_context* c, const void* G, void* Sigma, int solver, int precision, void* stream) {
+  return guarded(c, [&] {
+    if (!G || !Sigma) throw Error(GG_ERR_ARG, "gw: NULL buffer");
+    if (((reinterpret_cast<uintptr_t>(G) | reinterpret_cast<uintptr_t>(Sigma)) & 15) != 0)
+      throw Error(GG_ERR_ARG, "gw: device buffers must be 16-byte aligned");
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    gw_build(c, (const double2*)G, (double2*)Sigma, solver, precision, st);
+  });
+}
+
+int gg_gw_sigma(gg_context* c, const double* G, double* Sigma, int solver, int precision) {
+  return guarded(c, [&] {
+    if (!G || !Sigma) throw Error(GG_ERR_ARG, "gw: NULL buffer");
+    const auto& s = c->sh;
+    const size_t count = (size_t)s.nts * s.ns * s.ink * s.nao * s.nao;
+    double2* gin = c->G_in.ensure(count);
+    double2* sout = c->Sigma_out.ensure(count);
+    cudaEvent_t e0, e1;
+    GG_CUDA(cudaEventCreate(&e0));
+    GG_CUDA(cudaEventCreate(&e1));
+    GG_CUDA(cudaEventRecord(e0, c->stream));
+    GG_CUDA(cudaMemcpyAsync(gin, G, count * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    gw_build(c, gin, sout, solver, precision, c->stream);
+    GG_CUDA(cudaMemcpyAsync(Sigma, sout, count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA(cudaEventRecord(e1, c->stream));
+    GG_CUDA(cudaStreamSynchronize(c->stream));
+    float ms = 0;
+    GG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    c->last.e2e = ms * 1e-3;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  });
+}
+
+int gg_hf_exchange(gg_context* c, const double* dm, double* K_out) {
+  return guarded(c, [&] {
+    if (!dm || !K_out) throw Error(GG_ERR_ARG, "hf: NULL buffer");
+    const auto& s = c->sh;
+    const size_t count = (size_t)s.ns * s.ink * s.nao * s.nao;
+    double2* din = c->G_in.ensure(std::max(count, c->G_in.n));
+    double2* kout = c->hf_F.ensure(count);
+    GG_CUDA(cudaMemcpyAsync(din, dm, count * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    hf_exchange(c, din, kout, c->stream);
+    GG_CUDA(cudaMemcpyAsync(K_out, kout, count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int gg_hf_fock(gg_context* c, const double* dm, const double* S_k, double madelung, double* F_out) {
+  return guarded(c, [&] {
+    if (!dm || !S_k || !F_out) throw Error(GG_ERR_ARG, "hf: NULL buffer");
+    const auto& s = c->sh;
+    const int n = s.nao;
+    const size_t nn = (size_t)n * n, count = (size_t)s.ns * s.ink * nn;
+    double2* din = c->G_in.ensure(std::max(count, c->G_in.n));
+    double2* fout = c->hf_F.ensure(count);
+    GG_CUDA(cudaMemcpyAsync(din, dm, count * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    hf_exchange(c, din, fout, c->stream);
+    hf_direct(c, fout, c->stream);
+    std::vector<double2> F(count);
+    GG_CUDA(cudaMemcpyAsync(F.data(), fout, count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA(cudaStreamSynchronize(c->stream));
+    // Ewald: F -= c * madelung * S D S per (s, IBZ k), c = 0.5 (ns = 1) or 1 (hf_gpu_kernel.cpp:188-201)
+    const double pre = (s.ns == 2 ? 1.0 : 0.5) * madelung;
+    const double2* S = (const double2*)S_k;
+    const double2* D = (const double2*)dm;
+    std::vector<double2> tmp(nn);
+    for (size_t b = 0; b < (size_t)s.ns * s.ink; ++b) {
+      const double2* Sb = S + b * nn;
+      const double2* Db = D + b * nn;
+      for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+          double2 acc = make_double2(0, 0);
+          for (int a = 0; a < n; ++a) acc = cadd(acc, cmul(Sb[i * n + a], Db[a * n + j]));
+          tmp[i * n + j] = acc;
+        }
+      for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+          double2 acc = make_double2(0, 0);
+          for (int a = 0; a < n; ++a) acc = cadd(acc, cmul(tmp[i * n + a], Sb[a * n + j]));
+          F[b * nn + i * n + j] = csub(F[b * nn + i * n + j], cscale(acc, pre));
+        }
+    }
+    std::memcpy(F_out, F.data(), count * sizeof(double2));
+  });
+}
+
+int gg_symmetry_unfold(gg_context* c, const double* X_ibz, int64_t nmat, double* X_full) {
+  return guarded(c, [&] {
+    if (!X_ibz || !X_full || nmat <= 0) throw Error(GG_ERR_ARG, "unfold: bad arguments");
+    if (!c->has_sym) throw Error(GG_ERR_STATE, "unfold: symmetry not set");
+    const auto& s = c->sh;
+    const size_t nn = (size_t)s.nao * s.nao;
+    const size_t in_count = (size_t)nmat * s.ink * nn, out_count = (size_t)nmat * s.nk * nn;
+    DevBuf<double2> xin, xout;
+    xin.upload((const double2*)X_ibz, in_count, c->stream);
+    xout.ensure(out_count);
+    c->Gtmp.ensure(out_count);
+    unfold_matrices(c, xin.p, (int)nmat, 1, xout.p, c->stream);  // -> [k][m][n][n]
+    std::vector<double2> h(out_count);
+    GG_CUDA(cudaMemcpyAsync(h.data(), xout.p, out_count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA(cudaStreamSynchronize(c->stream));
+    double2* o = (double2*)X_full;
+    for (int k = 0; k < s.nk; ++k)
+      for (int64_t m = 0; m < nmat; ++m)
+        std::memcpy(o + ((size_t)m * s.nk + k) * nn, h.data() + ((size_t)k * nmat + m) * nn, nn * sizeof(double2));
+  });
+}
+
+int gg_set_profiling(gg_context* c, int enable) {
+  return guarded(c, [&] { c->profiling = enable != 0; });
+}
+
+int gg_kernel_stats(const gg_context* c, int which, int64_t* launches, double* seconds, double* flops) {
+  if (!c || which < 0 || which > 1) return GG_ERR_ARG;
+  if (launches) *launches = c->kstat_launches[which];
+  if (seconds) *seconds = c->kstat_seconds[which];
+  if (flops) *flops = c->kstat_flops[which];
+  return GG_OK;
+}
+
+int64_t gg_last_launch_count(const gg_context* c) { return c ? c->launches : 0; }
+
+int gg_last_timings(const gg_context* c, double* out, int n) {
+  if (!c || !out) return 0;
+  const double v[8] = {c->last.total, c->last.unfold, c->last.p0,    c->last.ir_fwd,
+                       c->last.dyson, c->last.ir_back, c->last.sigma, c->last.e2e};
+  int m = std::min(n, 8);
+  for (int i = 0; i < m; ++i) out[i] = v[i];
+  return m;
+}
+
+}  // extern "C"

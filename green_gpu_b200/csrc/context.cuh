@@ -1,0 +1,105 @@
+// Per-system device state behind the opaque gg_context of the C ABI.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace gg {
+
+// grow-only device buffer
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  T* ensure(size_t count) {
+    if (count > n) {
+      release();
+      if (count) GG_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+      n = count;
+    }
+    return p;
+  }
+  void upload(const T* host, size_t count, cudaStream_t st) {
+    ensure(count);
+    if (count) GG_CUDA(cudaMemcpyAsync(p, host, count * sizeof(T), cudaMemcpyHostToDevice, st));
+  }
+};
+
+struct Plan {
+  int qc = 1;   // irreducible q points per chunk
+  int kc = 1;   // k points per P0 chunk
+  int tb = 1;   // tau points per P0 batch
+  int dyson_batch = 1;  // Dyson systems per launch
+  size_t bytes = 0;
+};
+
+struct Timings {
+  double total = 0, unfold = 0, p0 = 0, ir_fwd = 0, dyson = 0, ir_back = 0, sigma = 0, e2e = 0;
+};
+
+}  // namespace gg
+
+struct gg_context {
+  gg_shape sh{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+
+  // symmetry (host copies + device copies of what kernels index)
+  bool has_sym = false;
+  std::vector<int64_t> k_f2r, k_r2f, k_tr, q_f2r, q_r2f, q_tr, k1_from_k2q, k2_from_k1q;
+  std::vector<std::vector<int>> k_stars, q_stars;
+  bool has_Uk = false, has_Uq = false;
+  gg::DevBuf<double2> Uk, Uq;
+  std::vector<double2> Uk_h;
+  gg::DevBuf<int> k_f2r_d, k_tr_d;
+
+  // k-pair store
+  bool has_kpairs = false;
+  int64_t nstored = 0;
+  std::vector<int64_t> conj_list, trans_list, irre_pos;
+  const double2* V = nullptr;  // device
+  gg::DevBuf<double2> V_owned;
+
+  // IR transforms
+  bool has_ir = false;
+  gg::DevBuf<double2> Ttn, Tnt_fold;
+
+  int slices = 4;
+  int shard_rank = 0, shard_size = 1;
+
+  // capture of intermediates (host pointers)
+  double* cap_P0 = nullptr;
+  double* cap_Pw = nullptr;
+  double* cap_Wt = nullptr;
+
+  // work buffers
+  gg::DevBuf<double2> G_in, Sigma_out, Gf, Gtmp, Vbuf, G1buf, scratchA, scratchB, P0buf, Pw, Afac, Wt, Wrot,
+      gemm_work, hf_D, hf_F, hf_c, hf_J;
+  gg::DevBuf<int> info, piv, idx_i;
+  gg::DevBuf<int64_t> pos_d;
+  gg::DevBuf<int> op_d;
+
+  gg::Timings last{};
+  long launches = 0;
+  bool profiling = false;
+  // per-kernel stats of the last build: [0] P0 contraction, [1] Sigma contraction
+  long kstat_launches[2] = {0, 0};
+  double kstat_seconds[2] = {0, 0};
+  double kstat_flops[2] = {0, 0};
+
+  ~gg_context() {
+    if (stream) cudaStreamDestroy(stream);
+  }
+};

@@ -1,0 +1,15 @@
+// Host orchestration entry points used by the C ABI (capi.cu).
+#pragma once
+
+#include "context.cuh"
+
+namespace gg {
+
+Plan plan_gw(gg_context* c);
+void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solver, int precision, cudaStream_t st);
+void hf_exchange(gg_context* c, const double2* dm_dev, double2* K_dev, cudaStream_t st);
+void hf_direct(gg_context* c, double2* F_dev, cudaStream_t st);
+void unfold_matrices(gg_context* c, const double2* X_in, int nouter, int ns, double2* out, cudaStream_t st);
+void kpair_op(const gg_context* c, int k1, int k2, int64_t* pos, int* op);
+
+}  // namespace gg

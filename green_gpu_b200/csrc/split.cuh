@@ -1,0 +1,15 @@
+// Split-precision (Ozaki-sliced INT8 tensor-core) complex GEMM for the dominant contractions.
+#pragma once
+
+#include "context.cuh"
+#include "zgemm.cuh"
+
+namespace gg {
+
+struct SplitGemm;
+// Per-context engine (workspace for slices); throws if the path is unavailable.
+SplitGemm* split_engine(gg_context* c);
+// Same contract as zgemm() for descriptors with KB >= 1; FP64 in, FP64 out.
+int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int slices, cudaStream_t st);
+
+}  // namespace gg

@@ -1,0 +1,283 @@
+// Batched complex FP64 GEMM engine (see zgemm.cuh).
+//
+// CTA tile 64 x 64 complex, K step 8 complex, 4 warps in a 2 x 2 layout, each warp a
+// 32 x 32 complex tile = 4 x 4 DMMA 8x8 tiles per real/imag plane.  Complex products use
+// four real DMMAs (rr, -ii, ri, ir) on fragments read with one 16-byte shared load each
+// (interleaved complex in shared memory).  Global->shared staging uses cp.async (16 B,
+// zero-fill at the edges) into a 3-stage ring; the shared layout follows the global
+// contiguity of each operand ([row][k] or [k][row]) with an XOR swizzle so both the async
+// copies and the fragment loads are bank-conflict free without padding.
+#include "zgemm.cuh"
+
+#include <algorithm>
+
+namespace gg {
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 8, NT = 128, STAGES = 3;
+constexpr int TILE = BM * BK;  // complex elements per operand stage
+static_assert(BM == BN, "square tiles assumed by the staging code");
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// swizzled position of tile element (row r, k) in a stage
+template <bool KMAJ>
+__device__ __forceinline__ int sidx(int r, int k) {
+  return KMAJ ? r * BK + (k ^ ((r & 1) << 2)) : k * BM + (r ^ ((k & 3) << 1));
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+template <bool A_K, bool B_K>
+__global__ void __launch_bounds__(NT, 2) zgemm_kernel(ZgemmDesc d, int tiles_m, int tiles_n) {
+  __shared__ __align__(16) double2 As[STAGES][TILE];
+  __shared__ __align__(16) double2 Bs[STAGES][TILE];
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+
+  const long bid = blockIdx.x;
+  const int ntile = tiles_m * tiles_n;
+  const int tile = (int)(bid % ntile);
+  const long rest = bid / ntile;
+  const int split = (int)(rest % d.splits);
+  const long batch = rest / d.splits;
+  const int b0 = (int)(batch % d.nb0);
+  const int b1 = (int)((batch / d.nb0) % d.nb1);
+  const int b2 = (int)(batch / ((long)d.nb0 * d.nb1));
+  const int tm = tile % tiles_m, tn = tile / tiles_m;
+  const int m0 = tm * BM, n0 = tn * BN;
+
+  const double2* Ab = d.A + b0 * d.a_b0 + b1 * d.a_b1 + b2 * d.a_b2;
+  const double2* Bb = d.B + b0 * d.b_b0 + b1 * d.b_b1 + b2 * d.b_b2;
+
+  // staging assignment: 512 elements per operand stage, 4 per thread
+  //   KMAJ : k = tid % 8, rows tid / 8 + 16 i
+  //   !KMAJ: row = tid % 64, k = tid / 64 + 2 i
+  long a_off[4], b_off[4];
+  bool a_ok[4], b_ok[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int ra = A_K ? tid / 8 + 16 * i : tid % 64;
+    const int m = m0 + ra;
+    a_ok[i] = m < d.M;
+    a_off[i] = a_ok[i] ? d.a_m(m) : 0;
+    const int rb = B_K ? tid / 8 + 16 * i : tid % 64;
+    const int n = n0 + rb;
+    b_ok[i] = n < d.N;
+    b_off[i] = b_ok[i] ? d.b_n(n) : 0;
+  }
+
+  const int ktiles = (d.K + BK - 1) / BK;
+  const long total = (long)d.KB * ktiles;
+  const long t_begin = total * split / d.splits;
+  const long t_end = total * (split + 1) / d.splits;
+
+  auto issue = [&](long t, int st) {
+    const int kb = (int)(t / ktiles);
+    const int k0 = (int)(t % ktiles) * BK;
+    const double2* Ak = Ab + kb * d.a_kb;
+    const double2* Bk = Bb + kb * d.b_kb;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = A_K ? tid / 8 + 16 * i : tid % 64;
+      const int kk = A_K ? tid % 8 : tid / 64 + 2 * i;
+      const int k = k0 + kk;
+      const bool v = a_ok[i] && k < d.K;
+      cp_async16(&As[st][sidx<A_K>(r, kk)], v ? (const void*)(Ak + a_off[i] + k * d.a_k) : (const void*)Ab, v);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = B_K ? tid / 8 + 16 * i : tid % 64;
+      const int kk = B_K ? tid % 8 : tid / 64 + 2 * i;
+      const int k = k0 + kk;
+      const bool v = b_ok[i] && k < d.K;
+      cp_async16(&Bs[st][sidx<B_K>(r, kk)], v ? (const void*)(Bk + b_off[i] + k * d.b_k) : (const void*)Bb, v);
+    }
+  };
+
+  double cr[4][4][2], ci[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      cr[a][b][0] = cr[a][b][1] = 0.0;
+      ci[a][b][0] = ci[a][b][1] = 0.0;
+    }
+
+  const double sa = d.conjA ? -1.0 : 1.0;
+  const double sb = d.conjB ? -1.0 : 1.0;
+  const int fr = lane >> 2, fk = lane & 3;
+
+  // prologue: STAGES-1 tiles in flight
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (t_begin + s < t_end) issue(t_begin + s, s);
+    cp_commit();
+  }
+  int st = 0;
+  for (long t = t_begin; t < t_end; ++t) {
+    cp_wait<STAGES - 2>();
+    __syncthreads();
+    // refill the stage consumed in the previous iteration
+    {
+      const long tn_ = t + STAGES - 1;
+      int sn = st + STAGES - 1;
+      if (sn >= STAGES) sn -= STAGES;
+      if (tn_ < t_end) issue(tn_, sn);
+      cp_commit();
+    }
+    const double2* as = As[st];
+    const double2* bs = Bs[st];
+#pragma unroll
+    for (int ks = 0; ks < BK / 4; ++ks) {
+      double ar[4], ai[4], an[4], br[4], bi[4];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt) {
+        const double2 v = as[sidx<A_K>(wm * 32 + mt * 8 + fr, ks * 4 + fk)];
+        ar[mt] = v.x;
+        ai[mt] = sa * v.y;
+        an[mt] = -ai[mt];
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const double2 v = bs[sidx<B_K>(wn * 32 + nt * 8 + fr, ks * 4 + fk)];
+        br[nt] = v.x;
+        bi[nt] = sb * v.y;
+      }
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          dmma(cr[mt][nt][0], cr[mt][nt][1], ar[mt], br[nt]);
+          dmma(cr[mt][nt][0], cr[mt][nt][1], an[mt], bi[nt]);
+          dmma(ci[mt][nt][0], ci[mt][nt][1], ar[mt], bi[nt]);
+          dmma(ci[mt][nt][0], ci[mt][nt][1], ai[mt], br[nt]);
+        }
+    }
+    st = (st + 1 == STAGES) ? 0 : st + 1;
+  }
+  cp_wait<0>();
+
+  // epilogue
+  const long batch_count = (long)d.nb0 * d.nb1 * d.nb2;
+  const double2* cbase = d.C + b0 * d.c_b0 + b1 * d.c_b1 + b2 * d.c_b2;
+  const bool use_beta = d.beta.x != 0.0 || d.beta.y != 0.0;
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt) {
+    const int m = m0 + wm * 32 + mt * 8 + fr;
+    if (m >= d.M) continue;
+    const long cm = d.c_m(m);
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int n = n0 + wn * 32 + nt * 8 + 2 * fk + j;
+        if (n >= d.N) continue;
+        const double2 acc = make_double2(cr[mt][nt][j], ci[mt][nt][j]);
+        if (d.splits > 1) {
+          d.work[((split * batch_count + batch) * d.M + m) * (long)d.N + n] = acc;
+        } else {
+          double2* c = const_cast<double2*>(cbase) + cm + d.c_n(n);
+          double2 v = cmul(d.alpha, acc);
+          if (use_beta) v = cadd(v, cmul(d.beta, *c));
+          *c = v;
+        }
+      }
+    }
+  }
+}
+
+__global__ void zgemm_reduce(ZgemmDesc d) {
+  const long batch_count = (long)d.nb0 * d.nb1 * d.nb2;
+  const long mn = (long)d.M * d.N;
+  const long total = batch_count * mn;
+  const bool use_beta = d.beta.x != 0.0 || d.beta.y != 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const long batch = i / mn;
+    const long e = i % mn;
+    const int m = (int)(e / d.N);
+    const int n = (int)(e % d.N);
+    double2 acc = make_double2(0.0, 0.0);
+    for (int s = 0; s < d.splits; ++s) acc = cadd(acc, d.work[(s * batch_count + batch) * mn + e]);
+    const int b0 = (int)(batch % d.nb0);
+    const int b1 = (int)((batch / d.nb0) % d.nb1);
+    const int b2 = (int)(batch / ((long)d.nb0 * d.nb1));
+    double2* c = d.C + b0 * d.c_b0 + b1 * d.c_b1 + b2 * d.c_b2 + d.c_m(m) + d.c_n(n);
+    double2 v = cmul(d.alpha, acc);
+    if (use_beta) v = cadd(v, cmul(d.beta, *c));
+    *c = v;
+  }
+}
+
+template <bool A_K, bool B_K>
+void launch(const ZgemmDesc& d, int tiles_m, int tiles_n, long blocks, cudaStream_t stream) {
+  zgemm_kernel<A_K, B_K><<<(unsigned)blocks, NT, 0, stream>>>(d, tiles_m, tiles_n);
+  GG_CHECK_LAUNCH();
+}
+
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    GG_CUDA(cudaGetDevice(&dev));
+    GG_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+  }
+  return n;
+}
+
+}  // namespace
+
+int zgemm(const ZgemmDesc& d0, cudaStream_t stream) {
+  ZgemmDesc d = d0;
+  if (d.M <= 0 || d.N <= 0 || d.nb0 <= 0 || d.nb1 <= 0 || d.nb2 <= 0) return 0;
+  if (d.K < 0 || d.KB < 1) throw Error(GG_ERR_ARG, "zgemm: bad K");
+  const int tiles_m = ceil_div(d.M, BM), tiles_n = ceil_div(d.N, BN);
+  const long batch = (long)d.nb0 * d.nb1 * d.nb2;
+  const long base = (long)tiles_m * tiles_n * batch;
+  // split-K when the grid under-fills the device and the reduction is long
+  int splits = 1;
+  const long ksteps = (long)d.KB * ceil_div(d.K, BK);
+  const long target = 2L * sm_count();
+  if (d.work && base < target && ksteps >= 32) {
+    splits = (int)std::min<long>((target + base - 1) / base, ksteps / 16);
+    const long need = (long)d.M * d.N * batch;
+    if (need > 0) splits = (int)std::min<long>(splits, d.work_elems / need);
+    splits = std::max(1, std::min(splits, 64));
+  }
+  d.splits = splits;
+  const long blocks = base * splits;
+  if (blocks > 0x7fffffffL) throw Error(GG_ERR_ARG, "zgemm: grid too large");
+  const bool ak = (d.a_k == 1), bk = (d.b_k == 1);
+  if (ak && bk) launch<true, true>(d, tiles_m, tiles_n, blocks, stream);
+  else if (ak) launch<true, false>(d, tiles_m, tiles_n, blocks, stream);
+  else if (bk) launch<false, true>(d, tiles_m, tiles_n, blocks, stream);
+  else launch<false, false>(d, tiles_m, tiles_n, blocks, stream);
+  int launches = 1;
+  if (splits > 1) {
+    const long total = (long)d.M * d.N * batch;
+    const int threads = 256;
+    const long nblk = std::min<long>((total + threads - 1) / threads, 65535L * 8);
+    zgemm_reduce<<<(unsigned)nblk, threads, 0, stream>>>(d);
+    GG_CHECK_LAUNCH();
+    ++launches;
+  }
+  return launches;
+}
+
+}  // namespace gg

@@ -1,0 +1,167 @@
+/*
+ * green-b200: B200-native (sm_100a) HF-exchange and GW self-energy kernels.
+ *
+ * C ABI of libgreen_b200.so.  Plain pointers and sizes only; every function
+ * returns an int status (GG_OK = 0) and never lets a C++ exception cross the
+ * boundary.  Complex numbers are interleaved (re, im) double pairs, i.e. the
+ * memory layout of std::complex<double>; all tensors are row-major (C order),
+ * the layout the reference's ndarray/Eigen::RowMajor tensors use.
+ *
+ * Which reference interface each entry point replaces (paths relative to the
+ * Green-Phys/green-gpu tree):
+ *
+ *   gg_create / gg_destroy        kernel object lifetime behind the shared_ptr<void>
+ *                                 returned by custom_gw_kernel / custom_hf_kernel
+ *                                 (src/green/gpu/gpu_factory.h:47-89) and the device
+ *                                 set-up of cugw_utils / cuhf_utils
+ *                                 (src/cugw_utils.cu:27-75, src/cuhf_utils.cu:31-72)
+ *   gg_set_symmetry               cu_symmetry::initialize (src/cu_symmetry.cu:36-140) fed
+ *                                 by make_cu_symmetry_data (src/gw_gpu_kernel.cpp:34-91)
+ *   gg_set_kpairs, gg_set_coulomb the integral store df_integral_t::read_entire /
+ *   gg_set_coulomb_device         symmetrize (src/green/gpu/df_integral_t.h:96-235)
+ *   gg_set_ir                     allocate_IR_transformation_matrices
+ *                                 (src/cuda_common.cu:93-108; Ttn_FB / Tnt_BF of
+ *                                 grids::transformer_t used at src/cugw_utils.cu:35)
+ *   gg_gw_sigma                   gw_gpu_kernel::solve (src/gw_gpu_kernel.cpp:163-205),
+ *                                 i.e. the callback of custom_gw_kernel
+ *                                 (src/green/gpu/gpu_factory.h:86-87)
+ *   gg_hf_exchange                cuhf_utils::accumulate_exchange_on_device
+ *                                 (src/cuhf_utils.cu:136-159)
+ *   gg_hf_fock                    hf_gpu_kernel::solve (src/hf_gpu_kernel.cpp:66-104),
+ *                                 i.e. the callback of custom_hf_kernel
+ *                                 (src/green/gpu/gpu_factory.h:50-61)
+ *   gg_symmetry_unfold            cu_symmetry::transform_k_ao_device
+ *                                 (src/cu_symmetry.cu:183-233)
+ */
+#ifndef GREEN_B200_H
+#define GREEN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define GG_OK 0
+#define GG_ERR_ARG 1       /* invalid argument or shape mismatch */
+#define GG_ERR_CUDA 2      /* CUDA runtime error (message has the call and file:line) */
+#define GG_ERR_NOT_HPD 3   /* Cholesky: I - P~ is not Hermitian positive definite */
+#define GG_ERR_SINGULAR 4  /* LU: exactly singular I - P~ */
+#define GG_ERR_STATE 5     /* a required input (symmetry, integrals, IR) was not set */
+#define GG_ERR_MEMORY 6    /* the system does not fit the device memory budget */
+#define GG_ERR_INTERNAL 7
+
+/* linear solver for (I - P~) W~ = P~ (LinearSolverType, src/green/gpu/common_defs.h:137-139) */
+#define GG_SOLVER_CHOLESKY 0
+#define GG_SOLVER_LU 1
+
+/* arithmetic of the contractions */
+#define GG_PREC_FP64 0     /* plain FP64 everywhere */
+#define GG_PREC_SPLIT 1    /* Ozaki-sliced INT8 tensor-core contractions, FP64 solve / IR / sums */
+
+typedef struct gg_context gg_context;
+
+typedef struct gg_shape {
+  int32_t nk;    /* full-BZ k points */
+  int32_t ink;   /* irreducible k points */
+  int32_t nq;    /* full-BZ q points (== nk) */
+  int32_t inq;   /* irreducible q points */
+  int32_t nao;   /* orbitals per spin block */
+  int32_t NQ;    /* auxiliary (density-fitting) basis size */
+  int32_t ns;    /* spins (1 or 2) */
+  int32_t nts;   /* imaginary-time points incl. 0 and beta; even */
+  int32_t nw_b;  /* bosonic Matsubara frequencies; nw_b <= nts */
+  int32_t reserved;
+} gg_shape;
+
+/* Create a context on CUDA device `device`.  Allocates no per-iteration state yet. */
+int gg_create(const gg_shape* shape, int device, gg_context** out);
+void gg_destroy(gg_context* ctx);
+/* Message of the last failing call on this context (or of the last failing gg_create on
+ * this thread when ctx is NULL).  Valid until the next call on the same context. */
+const char* gg_last_error(const gg_context* ctx);
+
+/* Symmetry tables (cu_symmetry_data, src/green/gpu/cu_symmetry.h:41-66).  All index
+ * arrays are int64.  k1_from_k2q / k2_from_k1q are flattened [k * nq + q].  U_k is
+ * complex [nk][nao][nao], U_q complex [nq][NQ][NQ]; pass NULL for identity rotations.
+ * Stars are the full-BZ points with the same reduced index, in ascending order. */
+int gg_set_symmetry(gg_context* ctx, const int64_t* k_full_to_reduced, const int64_t* k_reduced_to_full,
+                    const int64_t* k_tr_conj, const int64_t* q_full_to_reduced,
+                    const int64_t* q_reduced_to_full, const int64_t* q_tr_conj, const int64_t* k1_from_k2q,
+                    const int64_t* k2_from_k1q, const double* U_k, const double* U_q);
+
+/* k-pair store layout (df_integral_t.h:68-86, 153-173): for the triangular index
+ * idx = tri(k1 >= k2), conj_kpair_list[idx] / trans_kpair_list[idx] name the stored pair it
+ * is the conjugate / transpose of (== idx when none), irre_pos_kpair[idx] is the position
+ * of a stored pair in the V array (-1 otherwise).  Arrays have nk(nk+1)/2 entries. */
+int gg_set_kpairs(gg_context* ctx, int64_t num_kpair_stored, const int64_t* conj_kpair_list,
+                  const int64_t* trans_kpair_list, const int64_t* irre_pos_kpair);
+
+/* Density-fitted integrals V [num_kpair_stored][NQ][nao][nao] complex.  The host variant
+ * copies them into device memory owned by the context; the device variant borrows a
+ * device pointer that must stay valid for the context's lifetime. */
+int gg_set_coulomb(gg_context* ctx, const double* V_stored);
+int gg_set_coulomb_device(gg_context* ctx, const void* V_stored_device);
+
+/* IR transforms: Ttn_FB complex [nts][nw_b], Tnt_BF complex [nw_b][nts-2]. */
+int gg_set_ir(gg_context* ctx, const double* Ttn_FB, const double* Tnt_BF);
+
+/* Restrict the next GW builds to the irreducible q points iq with iq % size == rank (the
+ * round-robin distribution of src/cugw_utils.cu:115); the caller sums the partial Sigma
+ * over ranks (src/gw_gpu_kernel.cpp:187).  (0, 1) restores the full build. */
+int gg_set_q_shard(gg_context* ctx, int rank, int size);
+
+/* Number of Ozaki slices per operand for GG_PREC_SPLIT (2..8, default 4). */
+int gg_set_split_slices(gg_context* ctx, int slices);
+
+/* One GW self-energy build.  G_tskij complex [nts][ns][ink][nao][nao] (host), Sigma_tskij
+ * the same shape (host, overwritten: zeroed, accumulated, divided by nk as
+ * gw_gpu_kernel::solve does).  solver: GG_SOLVER_*; precision: GG_PREC_*. */
+int gg_gw_sigma(gg_context* ctx, const double* G_tskij, double* Sigma_tskij, int solver, int precision);
+/* Same with device buffers on the given cudaStream_t (NULL: the context's stream). */
+int gg_gw_sigma_device(gg_context* ctx, const void* G_tskij_device, void* Sigma_tskij_device, int solver,
+                       int precision, void* stream);
+
+/* Optional capture of intermediates of the next gg_gw_sigma* call (host pointers, any may
+ * be NULL): P0 [inq][nts][NQ][NQ] (scaled by 1/nk and mirrored), Pw [inq][nw_b][NQ][NQ]
+ * (Hermitian-symmetrised P~), Wt [inq][nts][NQ][NQ] (W~(tau)). */
+int gg_set_capture(gg_context* ctx, double* P0_out, double* Pw_out, double* Wt_out);
+
+/* Exchange part K_s(k) [ns][ink][nao][nao] for the IBZ density dm [ns][ink][nao][nao]
+ * (host buffers). */
+int gg_hf_exchange(gg_context* ctx, const double* dm, double* K_out);
+/* Full static self-energy of hf_gpu_kernel::solve: exchange (GPU) + direct + Ewald
+ * (S_k [ns][ink][nao][nao]).  Host buffers. */
+int gg_hf_fock(gg_context* ctx, const double* dm, const double* S_k, double madelung, double* F_out);
+
+/* X(k) = U_k X(k_ibz) U_k^+ (conjugated for time-reversal partners) for every full-BZ k:
+ * X_ibz [nmat][ink][nao][nao] -> X_full [nmat][nk][nao][nao]; host buffers. */
+int gg_symmetry_unfold(gg_context* ctx, const double* X_ibz, int64_t nmat, double* X_full);
+
+/* Seconds spent in each phase of the last GW build (device time, CUDA events):
+ * out[0] total, [1] G unfold, [2] P0, [3] IR forward, [4] Dyson, [5] IR back, [6] Sigma,
+ * [7] end to end of the last host-buffer call (gg_gw_sigma: H2D copy of G, build, D2H of
+ * Sigma).
+ * Returns the number of entries written (<= n). */
+int gg_last_timings(const gg_context* ctx, double* out, int n);
+
+/* Per-kernel device time of the last GW build, from CUDA events recorded around every
+ * launch of the named contraction on its stream when profiling is enabled:
+ * which = 0: the P0 contraction (sum over k of A_k B_k^T), 1: the Sigma contraction
+ * (W~ times (V G)).  Writes launches, total seconds and algorithmic flops
+ * (8MNK + 12MN per complex GEMM, src/green/gpu/common_defs.h:121-125). */
+int gg_set_profiling(gg_context* ctx, int enable);
+int gg_kernel_stats(const gg_context* ctx, int which, int64_t* launches, double* seconds, double* flops);
+/* Number of kernel launches issued by the last GW build or HF call. */
+int64_t gg_last_launch_count(const gg_context* ctx);
+
+/* Library build information string (static storage). */
+const char* gg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GREEN_B200_H */
