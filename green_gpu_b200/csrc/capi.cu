@@ -8,6 +8,8 @@
 #include "context.cuh"
 #include "engine.cuh"
 #include "kernels.cuh"
+#include "split.cuh"
+#include "zgemm.cuh"
 
 using namespace gg;
 
@@ -350,6 +352,36 @@ int gg_kernel_stats(const gg_context* c, int which, int64_t* launches, double* s
 }
 
 int64_t gg_last_launch_count(const gg_context* c) { return c ? c->launches : 0; }
+
+int gg_zgemm(gg_context* c, int64_t M, int64_t N, int64_t K, const double* A, const double* B, double* C,
+             int precision) {
+  return guarded(c, [&] {
+    if (!A || !B || !C || M <= 0 || N <= 0 || K <= 0) throw Error(GG_ERR_ARG, "zgemm: bad arguments");
+    DevBuf<double2> a, b, o;
+    a.upload((const double2*)A, (size_t)(M * K), c->stream);
+    b.upload((const double2*)B, (size_t)(K * N), c->stream);
+    o.ensure((size_t)(M * N));
+    ZgemmDesc d;
+    d.M = (int)M; d.N = (int)N; d.K = (int)K;
+    d.A = a.p; d.a_m.lo = K; d.a_k = 1;
+    d.B = b.p; d.b_k = N; d.b_n.lo = 1;
+    d.C = o.p; d.c_m.lo = N; d.c_n.lo = 1;
+    c->launches = 0;
+    if (precision == GG_PREC_SPLIT) {
+      c->launches += split_zgemm(split_engine(c), d, c->slices, c->stream);
+    } else if (precision == GG_PREC_FP64) {
+      DevBuf<double2> w;
+      d.work = w.ensure((size_t)1 << 20);
+      d.work_elems = 1 << 20;
+      c->launches += zgemm(d, c->stream);
+      GG_CUDA(cudaStreamSynchronize(c->stream));
+    } else {
+      throw Error(GG_ERR_ARG, "zgemm: unknown precision");
+    }
+    GG_CUDA(cudaMemcpyAsync(C, o.p, (size_t)(M * N) * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
 
 int gg_last_timings(const gg_context* c, double* out, int n) {
   if (!c || !out) return 0;

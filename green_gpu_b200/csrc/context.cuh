@@ -8,6 +8,9 @@
 
 namespace gg {
 
+struct SplitGemm;
+void split_release(SplitGemm* e);
+
 // grow-only device buffer
 template <typename T>
 struct DevBuf {
@@ -99,7 +102,10 @@ struct gg_context {
   double kstat_seconds[2] = {0, 0};
   double kstat_flops[2] = {0, 0};
 
+  gg::SplitGemm* split = nullptr;
+
   ~gg_context() {
+    if (split) gg::split_release(split);
     if (stream) cudaStreamDestroy(stream);
   }
 };

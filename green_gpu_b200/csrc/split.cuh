@@ -11,5 +11,6 @@ struct SplitGemm;
 SplitGemm* split_engine(gg_context* c);
 // Same contract as zgemm() for descriptors with KB >= 1; FP64 in, FP64 out.
 int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int slices, cudaStream_t st);
+void split_release(SplitGemm* e);
 
 }  // namespace gg

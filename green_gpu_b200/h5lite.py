@@ -1,13 +1,10 @@
-"""Minimal read-only HDF5 reader for the reference's test fixtures.
+"""Minimal read-only HDF5 reader (no libhdf5 / h5py dependency).
 
-Test-fixture tooling only: it is used by ``make_golden.py`` (in this folder) to
-turn the reference's HDF5 test data into small ``.npz`` golden files.  It
-supports exactly what those files use: superblock v0/v1, version-1 object
-headers, old-style (symbol-table) groups, fixed-point / floating-point /
-compound datatypes, and contiguous, compact or chunked (unfiltered) layouts.
+Reads the files green-mbpt writes for the density-fitted integrals and its inputs:
+superblock v0/v1, version-1 object headers, old-style (symbol-table) groups,
+fixed-point / floating-point / compound datatypes, and contiguous, compact or chunked
+(unfiltered) layouts.  Used by df_integral.py and by the golden-fixture script.
 """
-import struct
-
 import numpy as np
 
 
@@ -298,6 +295,3 @@ class H5File:
                 out.append(full)
         return out
 
-
-def struct_check():
-    return struct.calcsize("<Q") == 8

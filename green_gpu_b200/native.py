@@ -30,7 +30,7 @@ EXPORTS = [
     "gg_create", "gg_destroy", "gg_last_error", "gg_set_symmetry", "gg_set_kpairs", "gg_set_coulomb",
     "gg_set_coulomb_device", "gg_set_ir", "gg_set_split_slices", "gg_gw_sigma", "gg_gw_sigma_device",
     "gg_set_capture", "gg_hf_exchange", "gg_hf_fock", "gg_symmetry_unfold", "gg_last_timings", "gg_version",
-    "gg_set_profiling", "gg_kernel_stats", "gg_last_launch_count", "gg_set_q_shard",
+    "gg_set_profiling", "gg_kernel_stats", "gg_last_launch_count", "gg_set_q_shard", "gg_zgemm",
 ]
 
 
@@ -80,6 +80,7 @@ def load(path: str = LIB_PATH):
         "gg_kernel_stats": (C.c_int, [P, C.c_int, I64, D, D]),
         "gg_last_launch_count": (C.c_int64, [P]),
         "gg_set_q_shard": (C.c_int, [P, C.c_int, C.c_int]),
+        "gg_zgemm": (C.c_int, [P, C.c_int64, C.c_int64, C.c_int64, D, D, D, C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -233,6 +234,18 @@ class Context:
 
     def launch_count(self):
         return int(self.lib.gg_last_launch_count(self.h))
+
+    def zgemm(self, A, B, precision=PREC_FP64):
+        A = _c128(A)
+        B = _c128(B)
+        M, K = A.shape
+        K2, N = B.shape
+        if K != K2:
+            raise ValueError("inner dimensions differ")
+        out = np.empty((M, N), np.complex128)
+        self._check(self.lib.gg_zgemm(self.h, M, N, K, _d(A.view(np.float64)), _d(B.view(np.float64)),
+                                      _d(out.view(np.float64)), int(precision)))
+        return out
 
     def timings(self):
         buf = np.zeros(8)

@@ -157,6 +157,14 @@ int gg_kernel_stats(const gg_context* ctx, int which, int64_t* launches, double*
 /* Number of kernel launches issued by the last GW build or HF call. */
 int64_t gg_last_launch_count(const gg_context* ctx);
 
+/* Dense complex GEMM with the library's engines: C = A B for row-major A [M][K],
+ * B [K][N], C [M][N] (host buffers).  precision GG_PREC_FP64 runs the FP64 tensor-core
+ * engine, GG_PREC_SPLIT the Ozaki INT8 engine with the context's slice count.  Same
+ * arithmetic as the contractions inside gg_gw_sigma / gg_hf_exchange (no reference
+ * counterpart: it exposes the engine for accuracy studies). */
+int gg_zgemm(gg_context* ctx, int64_t M, int64_t N, int64_t K, const double* A, const double* B, double* C,
+             int precision);
+
 /* Library build information string (static storage). */
 const char* gg_version(void);
 

@@ -147,17 +147,19 @@ def rotate_w(sys_, Wt, q_deg):
     return out
 
 
-def gw_build(sys_, solver="cholesky", keep=None):
+def gw_build(sys_, solver="cholesky", keep=None, q_subset=None):
     """Full GW self-energy build; returns Sigma [nts][ns][ink][nao][nao] (already / nk).
 
     src/cugw_utils.cu:104-202 for the q loop, src/gw_gpu_kernel.cpp:185-188 for / nk.
     If ``keep`` is a dict, intermediates P0 [inq][nts][NQ][NQ], Pw, Wt are stored in it.
+    ``q_subset`` restricts the irreducible q points (one device rank's share,
+    cugw_utils.cu:115); the partial results of all ranks sum to the full Sigma.
     """
     Gf = g_full(sys_)
     Sigma = np.zeros((sys_.nts, sys_.ns, sys_.ink, sys_.nao, sys_.nao), np.complex128)
     if keep is not None:
         keep["P0"], keep["Pw"], keep["Wt"] = [], [], []
-    for iq in range(sys_.inq):
+    for iq in (range(sys_.inq) if q_subset is None else q_subset):
         q_ir = sys_.q_reduced_to_full[iq]
         P0 = scale_mirror(p0_q(sys_, Gf, q_ir), sys_.nk, sys_.nts)
         Pw = transform_tw(P0, sys_.Tnt_BF)

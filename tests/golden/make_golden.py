@@ -18,8 +18,8 @@ import sys
 
 import numpy as np
 
-sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
-from h5lite import H5File  # noqa: E402
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+from green_gpu_b200.h5lite import H5File  # noqa: E402
 
 
 def main(ref_root="/root/reference"):

@@ -119,3 +119,14 @@ def test_hermitian_symmetrize_matches_reference_kernel():
             R[i, j] = re + 1j * im
             R[j, i] = re - 1j * im
     assert np.array_equal(gw.hermitian_symmetrize(M), R)
+
+
+def test_df_integral_reader_matches_fixture():
+    import os
+    ref_dir = "/root/reference/test/data/HF/df_hf_int"
+    if not os.path.isdir(ref_dir):
+        pytest.skip("reference tree not mounted")
+    from green_gpu_b200 import df_integral
+    s, _ = fixture.load()
+    V = df_integral.read_stored(ref_dir, s.nao, s.NQ)
+    assert np.array_equal(V, s.V_stored)
