@@ -50,6 +50,8 @@ void check_shape(const gg_shape& s) {
 
 }  // namespace
 
+void gg::set_thread_error(const std::string& msg) { g_create_error = msg; }
+
 extern "C" {
 
 const char* gg_version(void) { return "green-b200 0.1 (sm_100a; FP64 DMMA engine)"; }

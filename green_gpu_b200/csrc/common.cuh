@@ -40,4 +40,7 @@ __host__ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {
 
 inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
 
+// message returned by gg_last_error(NULL) on this thread (capi.cu)
+void set_thread_error(const std::string& msg);
+
 }  // namespace gg

@@ -31,6 +31,7 @@ EXPORTS = [
     "gg_set_coulomb_device", "gg_set_ir", "gg_set_split_slices", "gg_gw_sigma", "gg_gw_sigma_device",
     "gg_set_capture", "gg_hf_exchange", "gg_hf_fock", "gg_symmetry_unfold", "gg_last_timings", "gg_version",
     "gg_set_profiling", "gg_kernel_stats", "gg_last_launch_count", "gg_set_q_shard", "gg_zgemm",
+    "gg_zgemm_noalloc",
 ]
 
 
@@ -81,6 +82,7 @@ def load(path: str = LIB_PATH):
         "gg_last_launch_count": (C.c_int64, [P]),
         "gg_set_q_shard": (C.c_int, [P, C.c_int, C.c_int]),
         "gg_zgemm": (C.c_int, [P, C.c_int64, C.c_int64, C.c_int64, D, D, D, C.c_int]),
+        "gg_zgemm_noalloc": (C.c_int, [C.c_int64, C.c_int64, C.c_int64, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -79,8 +79,9 @@ typedef struct gg_shape {
 /* Create a context on CUDA device `device`.  Allocates no per-iteration state yet. */
 int gg_create(const gg_shape* shape, int device, gg_context** out);
 void gg_destroy(gg_context* ctx);
-/* Message of the last failing call on this context (or of the last failing gg_create on
- * this thread when ctx is NULL).  Valid until the next call on the same context. */
+/* Message of the last failing call on this context (or, when ctx is NULL, of the last
+ * failing context-free call on this thread: gg_create or gg_zgemm_noalloc).  Valid until
+ * the next call on the same context / thread. */
 const char* gg_last_error(const gg_context* ctx);
 
 /* Symmetry tables (cu_symmetry_data, src/green/gpu/cu_symmetry.h:41-66).  All index
@@ -164,6 +165,23 @@ int64_t gg_last_launch_count(const gg_context* ctx);
  * counterpart: it exposes the engine for accuracy studies). */
 int gg_zgemm(gg_context* ctx, int64_t M, int64_t N, int64_t K, const double* A, const double* B, double* C,
              int precision);
+
+/* C = A B for device buffers A [M][K], B [K][N], C [M][N] (row-major complex128, 16-byte
+ * aligned), FP64 tensor-core engine, enqueued on `stream` (a cudaStream_t; NULL = legacy
+ * default stream) without synchronising.  No counterpart in the reference: this entry
+ * point exists for callers that may not allocate device memory where they call it - code
+ * running while a CUDA graph is captured, programs whose device memory belongs to another
+ * allocator or to a budget fixed at start-up, and latency-bound loops in which cudaMalloc's
+ * implicit device synchronisation would stall other streams.  It allocates nothing: the
+ * split-K partial sums live in a static 16 MiB device array (2^20 complex numbers) that
+ * every GPU loading this library keeps until the process exits, so M * N may not exceed
+ * 2^19 (larger sizes return GG_ERR_ARG with the limit in gg_last_error(NULL)).  The first
+ * call on each device looks the array's address up once (cudaGetSymbolAddress with that
+ * device current); make that first call before any stream capture.  All calls share the
+ * array and every value a call reads from it was written earlier in the same call, so
+ * nothing needs clearing - but calls that overlap on the GPU (different streams, or
+ * different host threads on one device) race on it and must be serialised by the caller. */
+int gg_zgemm_noalloc(int64_t M, int64_t N, int64_t K, const void* A, const void* B, void* C, void* stream);
 
 /* Library build information string (static storage). */
 const char* gg_version(void);
