@@ -184,7 +184,8 @@ def run_reference(args):
     v = len(timed) / sum(timed)
     line = {"metric": "GW Sigma builds/s", "value": v, "unit": "builds/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(timed) / len(timed),
-            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "c128",
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "c128" if args.precision == "fp64" else "c128 in/out, int8 slices on tensor cores",
             "data": "synthetic", "impl": "reference",
             "config": {"workload": f"GW Sigma build, {args.config}", **{k: str(v_) for k, v_ in CONFIGS[args.config].items()}},
             "cpu_baseline": {**{k: cb[k] for k in ("unit", "cores", "kind", "sample")}, "value": v},
@@ -196,11 +197,12 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="cfg2", choices=sorted(CONFIGS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
+    ap.add_argument("--precision", default="split", choices=["fp64", "split"])
+    ap.add_argument("--slices", type=int, default=5)
     ap.add_argument("--solver", default="cholesky", choices=["cholesky", "lu"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -231,6 +233,7 @@ def main():
     ctx.set_coulomb_device(V.data_ptr(), V)
     ctx.set_ir(s.Ttn_FB, s.Tnt_BF)
     ctx.set_q_shard(rank, world)
+    ctx.set_split_slices(args.slices)
     prec = native.PREC_SPLIT if args.precision == "split" else native.PREC_FP64
     solver = native.SOLVER_CHOLESKY if args.solver == "cholesky" else native.SOLVER_LU
     G_host = torch.from_numpy(s.G_tskij.view(np.float64)).pin_memory()
@@ -298,13 +301,22 @@ def main():
     n_l, sec, fl = kstats[dom]
     achieved = fl / sec / 1e12 if sec > 0 else 0.0
     fp64_peak = float(os.environ.get("GG_FP64_PEAK_TFLOPS", "40.0"))
+    kname = "p0_contraction" if dom == 0 else "sigma_contraction"
     if args.precision == "fp64":
         peak, peak_note = fp64_peak, "nominal FP64 tensor (DMMA) peak of B200; no measured FP64 figure"
+        unit = "TFLOP/s"
+        kname += " (FP64 DMMA zgemm)"
     else:
-        peak, peak_note = 2.0 * pk["bf16_tflops"], f"2x {pk_src} bf16 (dense INT8 rate)"
-    roof = {"bound": "tensor", "kernel": "p0_contraction" if dom == 0 else "sigma_contraction",
-            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
-            "traffic": None, "launches": n_l, "avg_launch_ms": 1e3 * sec / max(n_l, 1), "peak_source": peak_note}
+        # executed INT8 work: S(S+1)/2 slice pairs, each a real GEMM of 8MNK ops per complex GEMM
+        pairs = args.slices * (args.slices + 1) // 2
+        achieved *= pairs
+        peak, peak_note = 2.0 * pk["bf16_tflops"], f"2x {pk_src} bf16 burst (dense INT8 rate)"
+        unit = "TOP/s (int8)"
+        kname += f" (slicing + tcgen05 INT8 GEMM, {args.slices} slices)"
+    roof = {"bound": "tensor", "kernel": kname,
+            "achieved": achieved, "peak": peak, "unit": unit, "frac": achieved / peak if peak else None,
+            "traffic": None, "launches": n_l, "avg_launch_ms": 1e3 * sec / max(n_l, 1), "peak_source": peak_note,
+            "model_tflops": fl / sec / 1e12 if sec > 0 else None}
     traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(traffic_file):
         with open(traffic_file) as f:
@@ -316,10 +328,12 @@ def main():
     line = {
         "metric": "GW Sigma builds/s", "value": value, "unit": "builds/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
-        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "c128",
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "c128" if args.precision == "fp64" else "c128 in/out, int8 slices on tensor cores",
         "data": "synthetic (seeded G from random Hermitian Fock, Gaussian V*exp(-0.1Q))",
         "config": {"workload": f"GW Sigma build {args.config}", "mesh": "x".join(map(str, CONFIGS[args.config]["mesh"])),
                    "nao": s.nao, "NQ": s.NQ, "nts": s.nts, "nw_b": s.nw_b, "precision": args.precision,
+                   "slices": args.slices if args.precision == "split" else None,
                    "solver": args.solver, "l2": "inputs larger than L2 (V = %.1f GB)" % (V.numel() * 8 / 1e9),
                    "parallelism": f"q-shard x{world}" if world > 1 else "1 GPU"},
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
@@ -331,6 +345,17 @@ def main():
         "e2e": {"value": (1.0 / statistics.mean(e2e_t)) if e2e_t else None, "unit": "builds/s",
                 "h2d_bytes_per_step": gbytes, "d2h_bytes_per_step": gbytes},
     }
+    if rank == 0 and args.precision == "split":
+        # accuracy of the split path against FP64 on the 2x2x2 k, nao 26, NQ 120 system
+        from green_gpu_b200 import synth as _synth
+        s1 = _synth.make_system(seed=7, **CONFIGS["cfg1"])
+        c1 = native.context_for(s1, device=local)
+        c1.set_split_slices(args.slices)
+        r64 = c1.gw_sigma(s1.G_tskij, solver=solver, precision=native.PREC_FP64)
+        rsp = c1.gw_sigma(s1.G_tskij, solver=solver, precision=native.PREC_SPLIT)
+        line["accuracy"] = {"sigma_max_rel_err_vs_fp64": float(np.abs(rsp - r64).max() / np.abs(r64).max()),
+                            "system": "cfg1 (2x2x2 k, nao 26, NQ 120)", "slices": args.slices}
+        c1.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = oracle_cpu_baseline(args.config)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}

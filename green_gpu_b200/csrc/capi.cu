@@ -209,6 +209,13 @@ int gg_set_ir(gg_context* c, const double* Ttn_FB, const double* Tnt_BF) {
   });
 }
 
+int gg_set_hf_precision(gg_context* c, int precision) {
+  return guarded(c, [&] {
+    if (precision != GG_PREC_FP64 && precision != GG_PREC_SPLIT) throw Error(GG_ERR_ARG, "hf: unknown precision");
+    c->hf_precision = precision;
+  });
+}
+
 int gg_set_q_shard(gg_context* c, int rank, int size) {
   return guarded(c, [&] {
     if (size < 1 || rank < 0 || rank >= size) throw Error(GG_ERR_ARG, "q shard: need 0 <= rank < size");
@@ -371,6 +378,7 @@ int gg_zgemm(gg_context* c, int64_t M, int64_t N, int64_t K, const double* A, co
     c->launches = 0;
     if (precision == GG_PREC_SPLIT) {
       c->launches += split_zgemm(split_engine(c), d, c->slices, c->stream);
+      split_check(c->split, c->stream);
     } else if (precision == GG_PREC_FP64) {
       DevBuf<double2> w;
       d.work = w.ensure((size_t)1 << 20);
@@ -383,6 +391,29 @@ int gg_zgemm(gg_context* c, int64_t M, int64_t N, int64_t K, const double* A, co
     GG_CUDA(cudaMemcpyAsync(C, o.p, (size_t)(M * N) * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     GG_CUDA(cudaStreamSynchronize(c->stream));
   });
+}
+
+int gg_estimate_bytes(const gg_shape* shape, int64_t nstored, int64_t* bytes) {
+  if (!shape || !bytes || nstored < 0) return GG_ERR_ARG;
+  try {
+    check_shape(*shape);
+  } catch (const Error& e) {
+    g_create_error = e.what();
+    return e.code;
+  }
+  const auto& s = *shape;
+  const double z = 16.0;
+  const double nn = (double)s.nao * s.nao, NN = (double)s.NQ * s.NQ, Nnn = (double)s.NQ * nn;
+  const int T2 = s.nts / 2, tb = std::min(T2, 4);
+  double b = (double)nstored * Nnn;                    // V store
+  b += 2.0 * s.nk * s.ns * s.nts * nn;                 // G full BZ + rotation scratch
+  b += (double)s.nk * Nnn + (double)s.nk * T2 * nn;    // gathered V, G(k+q)
+  b += 2.0 * std::max((double)s.nk * tb * Nnn, (double)s.nts * std::max(Nnn, NN));
+  b += (double)s.inq * (T2 + s.nw_b + s.nts) * NN;     // P0, P~ / W(iW), W(tau)
+  b += std::min(592.0, (double)s.inq * s.nw_b) * NN;   // Dyson work space
+  b += (double)s.nts * NN + (double)(1 << 22);         // W rotation, split-K partials
+  *bytes = (int64_t)(b * z);
+  return GG_OK;
 }
 
 int gg_last_timings(const gg_context* c, double* out, int n) {

@@ -80,6 +80,7 @@ struct gg_context {
   gg::DevBuf<double2> Ttn, Tnt_fold;
 
   int slices = 4;
+  int hf_precision = GG_PREC_FP64;
   int shard_rank = 0, shard_size = 1;
 
   // capture of intermediates (host pointers)

@@ -457,14 +457,15 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
               d.nb0 = T; d.a_b0 = 0; d.b_b0 = nn; d.c_b0 = Nnn;
               gemm(d);
             }
-            // Z[t][Q][x] = sum_P W'[t][P][Q] Y1[t][P][x]; W' = conj(W) for TR partners
+            // Z[t][Q][x] = sum_P Y1[t][P][x] W'[t][P][Q]; W' = conj(W) for TR partners.
+            // Rows are x = (j, c) (the large operand, read once per column tile), columns Q.
             {
               ZgemmDesc d;
-              d.M = N; d.N = (int)nn; d.K = N;
-              d.A = W; d.a_m.lo = 1; d.a_k = N; d.conjA = trq ? 1 : 0;
-              d.B = SA; d.b_k = nn; d.b_n.lo = 1;
-              d.C = SB; d.c_m.lo = nn; d.c_n.lo = 1;
-              d.nb0 = T; d.a_b0 = NN; d.b_b0 = Nnn; d.c_b0 = Nnn;
+              d.M = (int)nn; d.N = N; d.K = N;
+              d.A = SA; d.a_m.lo = 1; d.a_k = nn;
+              d.B = W; d.b_k = N; d.b_n.lo = 1; d.conjB = trq ? 1 : 0;
+              d.C = SB; d.c_m.lo = 1; d.c_n.lo = nn;
+              d.nb0 = T; d.a_b0 = Nnn; d.b_b0 = NN; d.c_b0 = Nnn;
               gemm_main(d, 1);
             }
             // Sigma[t][sp][kr][j][i] += -1/nk sum_Q sum_c Z[t][Q][j][c] conj(V[Q][i][c])
@@ -487,6 +488,7 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
   }
   tm.end(h_total);
   GG_CUDA(cudaStreamSynchronize(st));
+  if (split) split_check(split, st);
   for (auto& e : kev) {
     float ms = 0;
     GG_CUDA(cudaEventElapsedTime(&ms, e.second.first, e.second.second));
@@ -551,6 +553,7 @@ void hf_exchange(gg_context* c, const double2* dm_dev, double2* K_dev, cudaStrea
         d.work = work; d.work_elems = (long)c->gemm_work.n;
         c->launches += zgemm(d, st);
         // K[sp][kr][j][i] += pref/nk sum_{kk,Q} sum_c X[kk][Q][j][c] conj(V[kk][Q][i][c])  (:127-131)
+        // (the dominant exchange contraction; split precision when requested)
         ZgemmDesc e;
         e.M = n; e.N = n; e.K = n; e.KB = kn * N;
         e.A = X; e.a_m.lo = n; e.a_k = 1; e.a_kb = nn;
@@ -559,10 +562,14 @@ void hf_exchange(gg_context* c, const double2* dm_dev, double2* K_dev, cudaStrea
         e.alpha = make_double2(pref / nk, 0.0);
         e.beta = make_double2(1.0, 0.0);
         e.work = work; e.work_elems = (long)c->gemm_work.n;
-        c->launches += zgemm(e, st);
+        if (c->hf_precision == GG_PREC_SPLIT)
+          c->launches += split_zgemm(split_engine(c), e, c->slices, st);
+        else
+          c->launches += zgemm(e, st);
       }
     }
   }
+  if (c->hf_precision == GG_PREC_SPLIT) split_check(c->split, st);
 }
 
 // Hartree (direct) term J(k) = sum_Q c_Q V^Q(k,k), c_Q = 1/nk sum_{s,k'} Tr(V^Q(k',k') D_s(k'))

@@ -124,6 +124,13 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int* r) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, int* r) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
 struct I8Args {
   int S;
   int rows_a_pad, rows_b_pad;  // per (batch, slice)
@@ -133,6 +140,7 @@ struct I8Args {
   int tiles_m, tiles_n, splits;
   int nb0, nb1;
   long batch;
+  long units;                  // tiles_m * tiles_n * splits * batch work units
   const int* ea;  // [batch][rows_a_pad]
   const int* eb;  // [batch][N]
   // output: workspace [split][batch][M][N] when splits > 1, else C through the maps
@@ -143,9 +151,38 @@ struct I8Args {
   double2 alpha, beta;
   int stages;
   int tmem_cols;
+  int nbuf;  // accumulator sets in TMEM (1 or 2)
   int* err;
 };
 
+struct Unit {
+  long batch;
+  int split, m0, n0, kb0, kb1;
+};
+
+__device__ __forceinline__ Unit unit_of(const I8Args& p, long u, int BN) {
+  Unit w;
+  const int ntile = p.tiles_m * p.tiles_n;
+  const int tile = (int)(u % ntile);
+  const long rest = u / ntile;
+  w.split = (int)(rest % p.splits);
+  w.batch = rest / p.splits;
+  w.m0 = (tile % p.tiles_m) * BM;
+  w.n0 = (tile / p.tiles_m) * BN;
+  w.kb0 = (int)((long)p.nkb * w.split / p.splits);
+  w.kb1 = (int)((long)p.nkb * (w.split + 1) / p.splits);
+  return w;
+}
+
+__device__ __forceinline__ bool seg_last(const Unit& w, int kb, int kcb) {
+  return (kb + 1 == w.kb1) || ((kb + 1) % kcb == 0);
+}
+
+// Persistent: one CTA per SM walks the work units u = blockIdx.x + i * gridDim.x.  The TMA
+// ring runs on across units; TMEM holds nbuf accumulator sets (S diagonals x BN columns
+// each).  With two sets, consecutive K segments alternate so that draining one overlaps the
+// MMAs of the next; with one set the tile is as wide as 512 / S columns allow, which halves
+// the operand bytes per MAC - the better trade when L2 bandwidth is the limit.
 template <int BN>
 __global__ void __launch_bounds__(NTHREADS, 1)
     i8_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, I8Args p) {
@@ -157,31 +194,22 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   uint8_t* sB = smem + p.stages * stA;
   uint64_t* full = (uint64_t*)(sB + p.stages * stB);
   uint64_t* empty = full + p.stages;
-  uint64_t* accf = empty + p.stages;
-  uint64_t* acce = accf + 1;
-  uint64_t* fin = acce + 1;
+  uint64_t* accf = empty + p.stages;   // [2]
+  uint64_t* acce = accf + 2;           // [2]
+  uint64_t* fin = acce + 2;
   uint32_t* tslot = (uint32_t*)(fin + 1);
   volatile int* err = p.err;
-
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  long bid = blockIdx.x;
-  const int ntile = p.tiles_m * p.tiles_n;
-  const int tile = (int)(bid % ntile);
-  const long rest = bid / ntile;
-  const int split = (int)(rest % p.splits);
-  const long batch = rest / p.splits;
-  const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
-  const int m0 = tm * BM, n0 = tn * BN;
-  const int kb0 = (int)((long)p.nkb * split / p.splits);
-  const int kb1 = (int)((long)p.nkb * (split + 1) / p.splits);
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < p.stages; ++i) {
       mbar_init(&full[i], 1);
       mbar_init(&empty[i], 1);
     }
-    mbar_init(accf, 1);
-    mbar_init(acce, 8);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 8);
+    }
     mbar_init(fin, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -194,63 +222,73 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
+  const uint32_t buf_cols = (uint32_t)(S * BN);
 
   if (warp == 0) {
     // ---------------- TMA producer
     if (lane == 0) {
-      const int rowA = (int)((batch * S) * p.rows_a_pad + m0);
-      const int rowB = (int)((batch * S) * p.rows_b_pad + n0);
-      int issued = 0;
-      for (int kb = kb0; kb < kb1; ++kb) {
-        const int it = kb - kb0, st = it % p.stages, round = it / p.stages;
-        if (!mbar_wait(&empty[st], (round & 1) ^ 1, err, 1)) break;
-        mbar_expect_tx(&full[st], (uint32_t)(stA + stB));
-        for (int s = 0; s < S; ++s) {
-          tma_load_2d(sA + st * stA + s * BM * KB, &tmA, kb * KB, rowA + s * p.rows_a_pad, &full[st]);
-          tma_load_2d(sB + st * stB + s * BN * KB, &tmB, kb * KB, rowB + s * p.rows_b_pad, &full[st]);
+      long it = 0;
+      bool ok = true;
+      for (long u = blockIdx.x; u < p.units && ok; u += gridDim.x) {
+        const Unit w = unit_of(p, u, BN);
+        const int rowA = (int)((w.batch * S) * p.rows_a_pad + w.m0);
+        const int rowB = (int)((w.batch * S) * p.rows_b_pad + w.n0);
+        for (int kb = w.kb0; kb < w.kb1; ++kb, ++it) {
+          const int st = (int)(it % p.stages);
+          const uint32_t round = (uint32_t)(it / p.stages);
+          if (!mbar_wait(&empty[st], (round & 1) ^ 1, err, 1)) { ok = false; break; }
+          mbar_expect_tx(&full[st], (uint32_t)(stA + stB));
+          for (int s = 0; s < S; ++s) {
+            tma_load_2d(sA + st * stA + s * BM * KB, &tmA, kb * KB, rowA + s * p.rows_a_pad, &full[st]);
+            tma_load_2d(sB + st * stB + s * BN * KB, &tmB, kb * KB, rowB + s * p.rows_b_pad, &full[st]);
+          }
         }
-        ++issued;
       }
       // on failure, let the copies already issued land before the CTA can exit
-      if (*err)
-        for (int it = std::max(0, issued - p.stages); it < issued; ++it)
-          mbar_wait(&full[it % p.stages], (it / p.stages) & 1, err, 16, false);
+      if (!ok)
+        for (long j = (it > p.stages ? it - p.stages : 0); j < it; ++j)
+          mbar_wait(&full[j % p.stages], (uint32_t)((j / p.stages) & 1), err, 16, false);
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer
     if (lane == 0) {
-      const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
-      int seg = 0;
+      const uint32_t idesc =
+          (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+      long it = 0, g = 0;
       bool ok = true;
-      for (int kb = kb0; kb < kb1 && ok; ++kb) {
-        const int it = kb - kb0, st = it % p.stages, round = it / p.stages;
-        const bool first_in_seg = (kb == kb0) || (kb % p.kcb == 0);
-        if (first_in_seg && seg > 0) {
-          if (!mbar_wait(acce, (seg - 1) & 1, err, 2)) { ok = false; break; }
-        }
-        if (!mbar_wait(&full[st], round & 1, err, 4)) { ok = false; break; }
-        tc_fence_after();
-        const uint8_t* a = sA + st * stA;
-        const uint8_t* b = sB + st * stB;
-        for (int d = 2; d <= S + 1; ++d) {
-          const uint32_t tacc = tmem + (uint32_t)((d - 2) * BN);
-          const int s_lo = d - S > 1 ? d - S : 1, s_hi = d - 1 < S ? d - 1 : S;
-          for (int s = s_lo; s <= s_hi; ++s) {
-            const int t = d - s;
-            const uint64_t da = sw64_desc(a + (s - 1) * BM * KB);
-            const uint64_t db = sw64_desc(b + (t - 1) * BN * KB);
+      for (long u = blockIdx.x; u < p.units && ok; u += gridDim.x) {
+        const Unit w = unit_of(p, u, BN);
+        for (int kb = w.kb0; kb < w.kb1 && ok; ++kb, ++it) {
+          const int st = (int)(it % p.stages);
+          const uint32_t round = (uint32_t)(it / p.stages);
+          const bool first_in_seg = (kb == w.kb0) || (kb % p.kcb == 0);
+          const int buf = (int)(g % p.nbuf);
+          if (first_in_seg && g >= p.nbuf) {
+            if (!mbar_wait(&acce[buf], (uint32_t)(((g / p.nbuf) - 1) & 1), err, 2)) { ok = false; break; }
+          }
+          if (!mbar_wait(&full[st], round & 1, err, 4)) { ok = false; break; }
+          tc_fence_after();
+          const uint8_t* a = sA + st * stA;
+          const uint8_t* b = sB + st * stB;
+          for (int d = 2; d <= S + 1; ++d) {
+            const uint32_t tacc = tmem + (uint32_t)buf * buf_cols + (uint32_t)((d - 2) * BN);
+            const int s_lo = d - S > 1 ? d - S : 1, s_hi = d - 1 < S ? d - 1 : S;
+            for (int s = s_lo; s <= s_hi; ++s) {
+              const int t = d - s;
+              const uint64_t da = sw64_desc(a + (s - 1) * BM * KB);
+              const uint64_t db = sw64_desc(b + (t - 1) * BN * KB);
 #pragma unroll
-            for (int kk = 0; kk < KB / 32; ++kk) {
-              const uint32_t accum = (first_in_seg && s == s_lo && kk == 0) ? 0u : 1u;
-              mma_i8(tacc, da + (uint64_t)(kk * 2), db + (uint64_t)(kk * 2), idesc, accum);
+              for (int kk = 0; kk < KB / 32; ++kk) {
+                const uint32_t accum = (first_in_seg && s == s_lo && kk == 0) ? 0u : 1u;
+                mma_i8(tacc, da + (uint64_t)(kk * 2), db + (uint64_t)(kk * 2), idesc, accum);
+              }
             }
           }
-        }
-        mma_commit(&empty[st]);
-        const bool last_in_seg = (kb + 1 == kb1) || ((kb + 1) % p.kcb == 0);
-        if (last_in_seg) {
-          mma_commit(accf);
-          ++seg;
+          mma_commit(&empty[st]);
+          if (seg_last(w, kb, p.kcb)) {
+            mma_commit(&accf[buf]);
+            ++g;
+          }
         }
       }
       // all MMAs issued by this thread complete before TMEM can be freed
@@ -263,48 +301,58 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const int row = q * 32 + lane;
     constexpr int HC = BN / 2;  // int32 columns per thread
     double acc[HC];
-#pragma unroll
-    for (int i = 0; i < HC; ++i) acc[i] = 0.0;
-    // count segments exactly as the MMA issuer does
-    int nseg = 0;
-    for (int kb = kb0; kb < kb1; ++kb)
-      if ((kb + 1 == kb1) || ((kb + 1) % p.kcb == 0)) ++nseg;
+    long g = 0;
     bool ok = true;
-    for (int g = 0; g < nseg; ++g) {
-      if (!mbar_wait(accf, g & 1, err, 8)) { ok = false; break; }
-      tc_fence_after();
-      for (int d = 2; d <= S + 1; ++d) {
-        const double scale = ldexp(1.0, -7 * d);
-        const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((d - 2) * BN + h * HC);
+    for (long u = blockIdx.x; u < p.units && ok; u += gridDim.x) {
+      const Unit w = unit_of(p, u, BN);
 #pragma unroll
-        for (int j = 0; j < HC / 16; ++j) {
-          int r[16];
-          tmem_ld16(base + j * 16, r);
+      for (int i = 0; i < HC; ++i) acc[i] = 0.0;
+      for (int kb = w.kb0; kb < w.kb1; ++kb) {
+        if (!seg_last(w, kb, p.kcb)) continue;
+        const int buf = (int)(g % p.nbuf);
+        if (!mbar_wait(&accf[buf], (uint32_t)((g / p.nbuf) & 1), err, 8)) { ok = false; break; }
+        tc_fence_after();
+        for (int d = 2; d <= S + 1; ++d) {
+          const double scale = ldexp(1.0, -7 * d);
+          const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)buf * buf_cols +
+                                (uint32_t)((d - 2) * BN + h * HC);
 #pragma unroll
-          for (int i = 0; i < 16; ++i) acc[j * 16 + i] += (double)r[i] * scale;
+          for (int j = 0; j < HC / 16; ++j) {
+            int r[16];
+            tmem_ld16(base + j * 16, r);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc[j * 16 + i] += (double)r[i] * scale;
+          }
+          if constexpr (HC % 16 == 8) {
+            // BN = 48 / 80: the last 8 columns of the half
+            int r[8];
+            tmem_ld8(base + (HC / 16) * 16, r);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) acc[(HC / 16) * 16 + i] += (double)r[i] * scale;
+          }
         }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acce[buf]);
+        ++g;
       }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(acce);
-    }
-    if (ok && !*err) {
-      const int m = m0 + row;
+      if (!ok || *err) break;
+      const int m = w.m0 + row;
       if (m < p.M) {
-        const int ea = p.ea[batch * p.rows_a_pad + m];
-        const long batch_count = p.batch;
-        const int b0 = (int)(batch % p.nb0);
-        const int b1 = (int)((batch / p.nb0) % p.nb1);
-        const int b2 = (int)(batch / ((long)p.nb0 * p.nb1));
+        const int ea = p.ea[w.batch * p.rows_a_pad + m];
+        const int b0 = (int)(w.batch % p.nb0);
+        const int b1 = (int)((w.batch / p.nb0) % p.nb1);
+        const int b2 = (int)(w.batch / ((long)p.nb0 * p.nb1));
         const bool use_beta = p.beta.x != 0.0 || p.beta.y != 0.0;
+        const int nbase = (w.n0 + h * HC) / 2;
 #pragma unroll
         for (int c = 0; c < HC / 2; ++c) {
-          const int n = (n0 + h * HC) / 2 + c;
+          const int n = nbase + c;
           if (n < p.N) {
-            const int e = ea + p.eb[batch * p.N + n];
-            double2 v = make_double2(ldexp(acc[2 * c], e), ldexp(acc[2 * c + 1], e));
+            const int e = ea + __ldg(&p.eb[w.batch * p.N + n]);
+            const double2 v = make_double2(ldexp(acc[2 * c], e), ldexp(acc[2 * c + 1], e));
             if (p.splits > 1) {
-              p.work[((split * batch_count + batch) * p.M + m) * (long)p.N + n] = v;
+              p.work[((w.split * p.batch + w.batch) * p.M + m) * (long)p.N + n] = v;
             } else {
               double2* cp = p.C + b0 * p.c_b0 + b1 * p.c_b1 + b2 * p.c_b2 + p.c_m(m) + p.c_n(n);
               double2 o = cmul(p.alpha, v);
@@ -360,6 +408,25 @@ __global__ void row_exponent_kernel(OpView v, int rows_pad, int* out, long nbatc
   }
   for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   if (lane == 0) out[gw] = mx > 0.0 ? ilogb(mx) + 1 : 0;
+}
+
+// same, for operands whose rows are contiguous in memory: one thread per row, loop over k
+// (consecutive threads read consecutive addresses)
+__global__ void row_exponent_rc_kernel(OpView v, int rows_pad, int* out, long nbatch) {
+  const long gt = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (gt >= nbatch * rows_pad) return;
+  const long b = gt / rows_pad;
+  const int r = (int)(gt % rows_pad);
+  double mx = 0.0;
+  if (r < v.R) {
+    const double2* base = v.ptr(b) + v.rmap(r);
+    for (int kb = 0; kb < v.KB; ++kb)
+      for (int k = 0; k < v.K; ++k) {
+        const double2 x = base[kb * v.kbs + (long)k * v.ks];
+        mx = fmax(mx, fmax(fabs(x.x), fabs(x.y)));
+      }
+  }
+  out[gt] = mx > 0.0 ? ilogb(mx) + 1 : 0;
 }
 
 // cut x (|x| < 1 after scaling) into S int8 slices by truncation
@@ -519,13 +586,17 @@ void split_release(SplitGemm* e) { delete e; }
 int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
   if (S < 2 || S > 8) throw Error(GG_ERR_ARG, "split: slices must be in [2, 8]");
   if (d.M <= 0 || d.N <= 0) return 0;
-  const int BN = S <= 4 ? 128 : 64;
+  // nbuf accumulator sets of S diagonals x BN columns must fit the 512 TMEM columns;
+  // BN <= 128 keeps the FP64 drain registers (BN / 2 per thread) in budget
+  const int nbuf = S <= 2 ? 2 : 1;
+  const int BN = S <= 4 ? 128 : S == 5 ? 96 : S == 6 ? 80 : 64;
+  const int bn_pad = BN * 64 / std::__gcd(BN, 64);  // keeps rows_b_pad / 2 a multiple of 32
   const long batch = (long)d.nb0 * d.nb1 * d.nb2;
   const long Ktot = (long)d.KB * d.K;
   const long kp = ((2 * Ktot + KB - 1) / KB) * KB;
   const int rows_a_pad = ((d.M + BM - 1) / BM) * BM;
   const int np = 2 * d.N;
-  const int rows_b_pad = ((np + BN - 1) / BN) * BN;  // B' rows (2 per complex column)
+  const int rows_b_pad = ((np + bn_pad - 1) / bn_pad) * bn_pad;  // B' rows (2 per complex column)
   const int ncol_pad = rows_b_pad / 2;                // complex columns incl. padding
   // exact int32 chunk: S * Kchunk * 127^2 < 2^31
   const long kchunk = std::max<long>(KB, ((2147483647L / (16129L * S)) / KB) * KB);
@@ -536,19 +607,27 @@ int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
   int8_t* b8 = e->b8.ensure((size_t)batch * S * rows_b_pad * kp);
   int* ea = e->ea.ensure((size_t)batch * rows_a_pad);
   int* eb = e->eb.ensure((size_t)batch * d.N);
-  int* err = e->err.ensure(1);
-  GG_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+  int* err = e->err.p;
+  if (!err) {
+    err = e->err.ensure(1);
+    GG_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+  }
 
   OpView va{d.A, d.a_m, d.a_kb, d.a_k, d.KB, d.K, d.M, d.nb0, d.nb1, d.a_b0, d.a_b1, d.a_b2, d.conjA};
   OpView vb{d.B, d.b_n, d.b_kb, d.b_k, d.KB, d.K, d.N, d.nb0, d.nb1, d.b_b0, d.b_b1, d.b_b2, d.conjB};
   int launches = 0;
   {
-    const long warps = batch * rows_a_pad;
-    row_exponent_kernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(va, rows_a_pad, ea, batch);
-    GG_CHECK_LAUNCH();
-    const long warpsb = batch * d.N;
-    row_exponent_kernel<<<(unsigned)((warpsb * 32 + 255) / 256), 256, 0, st>>>(vb, d.N, eb, batch);
-    GG_CHECK_LAUNCH();
+    auto exponents = [&](const OpView& v, int rows_pad, int* out) {
+      const bool rcontig = v.rmap.lo == 1 && v.ks != 1;
+      const long n = batch * rows_pad;
+      if (rcontig)
+        row_exponent_rc_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(v, rows_pad, out, batch);
+      else
+        row_exponent_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(v, rows_pad, out, batch);
+      GG_CHECK_LAUNCH();
+    };
+    exponents(va, rows_a_pad, ea);
+    exponents(vb, d.N, eb);
     const long ktiles = (kp / 2 + 31) / 32;
     slice_kernel<false><<<(unsigned)(ktiles * (rows_a_pad / 32) * batch), 256, 0, st>>>(va, S, rows_a_pad, kp, ea, a8,
                                                                                         batch);
@@ -585,23 +664,45 @@ int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
   a.alpha = d.alpha;
   a.beta = d.beta;
   a.err = err;
+  a.nbuf = nbuf;
   a.tmem_cols = 32;
-  while (a.tmem_cols < S * BN) a.tmem_cols *= 2;
+  while (a.tmem_cols < nbuf * S * BN) a.tmem_cols *= 2;
   const size_t stage_bytes = (size_t)S * (BM + BN) * KB;
   a.stages = (int)std::min<size_t>(4, (220 * 1024 - 2048) / stage_bytes);
   if (a.stages < 2) throw Error(GG_ERR_ARG, "split: stage does not fit shared memory");
   const size_t smem = a.stages * stage_bytes + 1024 + 256;
   const long base = (long)a.tiles_m * a.tiles_n * batch;
+  // split-K so that the units fill whole waves of persistent CTAs (each split keeps >= 8 K blocks)
   int splits = 1;
-  if (base < sms()) splits = (int)std::min<long>((sms() + base - 1) / base, std::max(1, nkb / 4));
+  {
+    const int smax = (int)std::max<long>(1, std::min<long>(nkb / 8, 64));
+    double best = 0.0;
+    for (int sp = 1; sp <= smax; ++sp) {
+      const long units = base * sp;
+      const long waves = (units + sms() - 1) / sms();
+      const double eff = (double)units / (double)(waves * sms());
+      // prefer fewer splits unless a larger count fills the machine noticeably better
+      if (eff > best + 0.05) {
+        best = eff;
+        splits = sp;
+      }
+      if (units >= 4L * sms()) break;
+    }
+  }
   const long need = (long)d.M * d.N * batch;
   if (splits > 1) {
     e->work.ensure((size_t)splits * need);
   }
   a.splits = splits;
   a.work = e->work.p;
-  if (BN == 128) launch_i8<128>(ta, tb, a, base * splits, smem, st);
-  else launch_i8<64>(ta, tb, a, base * splits, smem, st);
+  a.units = base * splits;
+  const long grid = std::min<long>(a.units, sms());
+  switch (BN) {
+    case 128: launch_i8<128>(ta, tb, a, grid, smem, st); break;
+    case 96: launch_i8<96>(ta, tb, a, grid, smem, st); break;
+    case 80: launch_i8<80>(ta, tb, a, grid, smem, st); break;
+    default: launch_i8<64>(ta, tb, a, grid, smem, st); break;
+  }
   ++launches;
   if (splits > 1) {
     const long total = need;
@@ -611,11 +712,19 @@ int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
     GG_CHECK_LAUNCH();
     ++launches;
   }
-  GG_CUDA(cudaMemcpyAsync(&e->err_host, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  return launches;
+}
+
+void split_check(SplitGemm* e, cudaStream_t st) {
+  if (!e || !e->err.p) return;
+  GG_CUDA(cudaMemcpyAsync(&e->err_host, e->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   GG_CUDA(cudaStreamSynchronize(st));
   const int h = e->err_host;
-  if (h) throw Error(GG_ERR_INTERNAL, "split GEMM: pipeline wait timed out (code " + std::to_string(h) + ")");
-  return launches;
+  if (h) {
+    GG_CUDA(cudaMemsetAsync(e->err.p, 0, sizeof(int), st));
+    GG_CUDA(cudaStreamSynchronize(st));
+    throw Error(GG_ERR_INTERNAL, "split GEMM: pipeline wait timed out (code " + std::to_string(h) + ")");
+  }
 }
 
 }  // namespace gg

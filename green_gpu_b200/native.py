@@ -31,7 +31,7 @@ EXPORTS = [
     "gg_set_coulomb_device", "gg_set_ir", "gg_set_split_slices", "gg_gw_sigma", "gg_gw_sigma_device",
     "gg_set_capture", "gg_hf_exchange", "gg_hf_fock", "gg_symmetry_unfold", "gg_last_timings", "gg_version",
     "gg_set_profiling", "gg_kernel_stats", "gg_last_launch_count", "gg_set_q_shard", "gg_zgemm",
-    "gg_zgemm_noalloc",
+    "gg_zgemm_noalloc", "gg_set_hf_precision", "gg_estimate_bytes",
 ]
 
 
@@ -83,6 +83,8 @@ def load(path: str = LIB_PATH):
         "gg_set_q_shard": (C.c_int, [P, C.c_int, C.c_int]),
         "gg_zgemm": (C.c_int, [P, C.c_int64, C.c_int64, C.c_int64, D, D, D, C.c_int]),
         "gg_zgemm_noalloc": (C.c_int, [C.c_int64, C.c_int64, C.c_int64, P, P, P, P]),
+        "gg_set_hf_precision": (C.c_int, [P, C.c_int]),
+        "gg_estimate_bytes": (C.c_int, [C.POINTER(Shape), C.c_int64, C.POINTER(C.c_int64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -169,6 +171,9 @@ class Context:
     def set_q_shard(self, rank: int, size: int):
         self._check(self.lib.gg_set_q_shard(self.h, int(rank), int(size)))
 
+    def set_hf_precision(self, precision: int):
+        self._check(self.lib.gg_set_hf_precision(self.h, int(precision)))
+
     def set_split_slices(self, slices: int):
         self._check(self.lib.gg_set_split_slices(self.h, int(slices)))
 
@@ -254,6 +259,17 @@ class Context:
         n = self.lib.gg_last_timings(self.h, _d(buf), 8)
         keys = ["total", "unfold", "p0", "ir_fwd", "dyson", "ir_back", "sigma", "e2e"]
         return dict(zip(keys[:n], buf[:n].tolist()))
+
+
+def estimate_bytes(nk, ink, inq, nao, NQ, ns, nts, nw_b, num_kpair_stored) -> int:
+    """Device bytes of a resident context of this shape (gg_estimate_bytes)."""
+    lib = load()
+    sh = Shape(nk, ink, nk, inq, nao, NQ, ns, nts, nw_b, 0)
+    out = C.c_int64()
+    rc = lib.gg_estimate_bytes(C.byref(sh), int(num_kpair_stored), C.byref(out))
+    if rc != GG_OK:
+        raise GreenError(rc, lib.gg_last_error(None).decode())
+    return int(out.value)
 
 
 def context_for(sys_, device=0, upload_V=True) -> Context:

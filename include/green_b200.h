@@ -130,6 +130,11 @@ int gg_gw_sigma_device(gg_context* ctx, const void* G_tskij_device, void* Sigma_
  * (Hermitian-symmetrised P~), Wt [inq][nts][NQ][NQ] (W~(tau)). */
 int gg_set_capture(gg_context* ctx, double* P0_out, double* Pw_out, double* Wt_out);
 
+/* Arithmetic of the HF exchange contraction for the next gg_hf_exchange / gg_hf_fock calls
+ * (GG_PREC_FP64 default, GG_PREC_SPLIT: Ozaki INT8 with the context's slice count).  The
+ * reference's HF path is FP64 only (cuhf_utils.cu). */
+int gg_set_hf_precision(gg_context* ctx, int precision);
+
 /* Exchange part K_s(k) [ns][ink][nao][nao] for the IBZ density dm [ns][ink][nao][nao]
  * (host buffers). */
 int gg_hf_exchange(gg_context* ctx, const double* dm, double* K_out);
@@ -182,6 +187,11 @@ int gg_zgemm(gg_context* ctx, int64_t M, int64_t N, int64_t K, const double* A, 
  * nothing needs clearing - but calls that overlap on the GPU (different streams, or
  * different host threads on one device) race on it and must be serialised by the caller. */
 int gg_zgemm_noalloc(int64_t M, int64_t N, int64_t K, const void* A, const void* B, void* C, void* stream);
+
+/* Device bytes a context of this shape needs when its integrals are resident and its GW
+ * work space is planned without chunking (V store of num_kpair_stored pairs + work space);
+ * context-free, allocates nothing.  Used for admission by memory footprint. */
+int gg_estimate_bytes(const gg_shape* shape, int64_t num_kpair_stored, int64_t* bytes);
 
 /* Library build information string (static storage). */
 const char* gg_version(void);
