@@ -10,8 +10,9 @@
 //   IR fwd   P~_q(iW) = Tnt_BF P0_q(tau), mirror folded in      (cugw_qpt.cu:179-191, 329-339)
 //   Dyson    W~ = (I - P~)^{-1} P~ per (q, W), FP64             (cugw_qpt.cu:223-322)
 //   IR back  W~_q(tau) = Ttn_FB W~_q(iW)                        (cugw_qpt.cu:341-358)
-//   Sigma    Sigma_k(tau) -= sum_q' (V G)(k-q') W~_q' V^+       (cugw_qkpt.cu:248-338,
-//            cugw_utils.cu:240-269)
+//   Sigma    Sigma_k(tau) -= sum_q' ((V W~_q') G(k-q')) V^+     (cugw_qkpt.cu:248-338,
+//            cugw_utils.cu:240-269; the reference forms V G first, here V W~ is formed
+//            first so that V is the tau- and spin-independent operand of the main GEMM)
 #include "engine.cuh"
 
 #include <algorithm>
@@ -142,7 +143,7 @@ void unfold_matrices(gg_context* c, const double2* X_in, int nouter, int ns, dou
   ++c->launches;
 }
 
-Plan plan_gw(gg_context* c) {
+Plan plan_gw(gg_context* c, int slices) {
   const auto& s = c->sh;
   const size_t z = sizeof(double2);
   const size_t nn = (size_t)s.nao * s.nao, NN = (size_t)s.NQ * s.NQ, Nnn = (size_t)s.NQ * nn;
@@ -158,7 +159,7 @@ Plan plan_gw(gg_context* c) {
     b += (size_t)q.kc * Nnn;                           // Vbuf
     b += (size_t)q.kc * T2 * nn;                       // G1buf
     size_t p0s = (size_t)q.kc * q.tb * Nnn;            // A / B build buffers (each)
-    size_t sgs = (size_t)s.nts * std::max(Nnn, NN);    // Sigma Y1 / Z, W rotation (each)
+    size_t sgs = (size_t)s.nts * std::max(Nnn, NN);    // Sigma X / Z, W rotation (each)
     b += 2 * std::max(p0s, sgs);
     b += (size_t)q.qc * T2 * NN;                       // P0
     b += (size_t)q.qc * s.nw_b * NN;                   // Pw
@@ -166,11 +167,29 @@ Plan plan_gw(gg_context* c) {
     b += (size_t)q.qc * s.nts * NN;                    // Wt
     b += (size_t)s.nts * NN;                           // Wrot
     b += (size_t)1 << 22;                              // split-K partials
-    return b * z;
+    b *= z;
+    if (slices > 0) {
+      // int8 slices of the P0 contraction operands (rows padded to the tile sizes), K = 2 nn kc bytes
+      b += (size_t)q.tb * slices * (size_t)(3 * s.NQ + 320) * 2 * nn * q.kc;
+    }
+    return b;
   };
   p.qc = s.inq;
   p.kc = s.nk;
-  p.tb = std::min(T2, 4);
+  // tau block of the P0 operand builds: rows (tt, a) of tb * nao, chosen to waste the least
+  // of the 64-row GEMM tiles over all tau blocks (largest such tb up to 12)
+  {
+    long best = -1;
+    p.tb = 1;
+    for (int tb = 1; tb <= std::min(T2, 12); ++tb) {
+      long padded = 0;
+      for (int t0 = 0; t0 < T2; t0 += tb) padded += 64L * ((std::min(tb, T2 - t0) * (long)s.nao + 63) / 64);
+      if (best < 0 || padded <= best) {
+        best = padded;
+        p.tb = tb;
+      }
+    }
+  }
   while (need(p) > budget) {
     if (p.qc > 1) p.qc = (p.qc + 1) / 2;
     else if (p.tb > 1) p.tb = (p.tb + 1) / 2;
@@ -191,7 +210,7 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
   const auto& s = c->sh;
   const int n = s.nao, N = s.NQ, T = s.nts, T2 = T / 2, nw = s.nw_b, nk = s.nk, ns = s.ns;
   const long nn = (long)n * n, NN = (long)N * N, Nnn = (long)N * nn;
-  const Plan pl = plan_gw(c);
+  const Plan pl = plan_gw(c, precision == GG_PREC_SPLIT ? c->slices : 0);
   c->launches = 0;
 
   // work buffers (sized before the first launch)
@@ -313,31 +332,31 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
           ++c->launches;
           for (int t0 = 0; t0 < T2; t0 += pl.tb) {
             const int tn = std::min(pl.tb, T2 - t0);
-            // A-build: SA[kk][tt][Q'][a][b] = sum_p G^k(tau_{T-1-t})[a][p] V[kk][Q'][p][b]
+            // A-build: SA[kk][tt][Q'][a][b] = sum_p G^k(tau_{T-1-t})[a][p] V[kk][Q'][p][b].
+            // The tau block is folded into the rows, m = (tt, a), so that V[kk] is one shared
+            // operand and the row tiles are full (n alone is below one tile).
             {
               ZgemmDesc d;
-              d.M = n; d.N = N * n; d.K = n;
+              d.M = tn * n; d.N = N * n; d.K = n;
               d.A = Gf + ((long)k0 * ns + sp) * T * nn + (long)(T - 1 - t0) * nn;
-              d.a_m.lo = n; d.a_k = 1;
+              d.a_m.split = n; d.a_m.hi = -nn; d.a_m.lo = n; d.a_k = 1;
               d.B = Vb; d.b_k = n; d.b_n.split = n; d.b_n.hi = nn; d.b_n.lo = 1;
-              d.C = SA; d.c_m.lo = n; d.c_n.split = n; d.c_n.hi = nn; d.c_n.lo = 1;
-              d.nb0 = tn; d.nb1 = kn;
-              d.a_b0 = -nn; d.a_b1 = (long)ns * T * nn;
-              d.b_b0 = 0; d.b_b1 = Nnn;
-              d.c_b0 = Nnn; d.c_b1 = (long)tn * Nnn;
+              d.C = SA; d.c_m.split = n; d.c_m.hi = Nnn; d.c_m.lo = n;
+              d.c_n.split = n; d.c_n.hi = nn; d.c_n.lo = 1;
+              d.nb0 = kn;
+              d.a_b0 = (long)ns * T * nn; d.b_b0 = Nnn; d.c_b0 = (long)tn * Nnn;
               gemm(d);
             }
-            // B-build: SB[kk][tt][Q][a][b] = sum_l conj(V[kk][Q][a][l]) G^{k+q}(tau_t)[b][l]
+            // B-build: SB[kk][tt][Q][a][b] = sum_l conj(V[kk][Q][a][l]) G^{k+q}(tau_t)[b][l],
+            // tau folded into the columns, n = (tt, b)
             {
               ZgemmDesc d;
-              d.M = N * n; d.N = n; d.K = n;
+              d.M = N * n; d.N = tn * n; d.K = n;
               d.A = Vb; d.a_m.lo = n; d.a_k = 1; d.conjA = 1;
-              d.B = G1 + (long)t0 * nn; d.b_k = 1; d.b_n.lo = n;
-              d.C = SB; d.c_m.lo = n; d.c_n.lo = 1;
-              d.nb0 = tn; d.nb1 = kn;
-              d.a_b0 = 0; d.a_b1 = Nnn;
-              d.b_b0 = nn; d.b_b1 = (long)T2 * nn;
-              d.c_b0 = Nnn; d.c_b1 = (long)tn * Nnn;
+              d.B = G1 + (long)t0 * nn; d.b_k = 1; d.b_n.split = n; d.b_n.hi = nn; d.b_n.lo = n;
+              d.C = SB; d.c_m.lo = n; d.c_n.split = n; d.c_n.hi = Nnn; d.c_n.lo = 1;
+              d.nb0 = kn;
+              d.a_b0 = Nnn; d.b_b0 = (long)T2 * nn; d.c_b0 = (long)tn * Nnn;
               gemm(d);
             }
             // P0[q][t] (+)= pref/nk sum_kk sum_x SA[kk][tt][Q'][x] SB[kk][tt][Q][x]
@@ -446,36 +465,38 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
           const int k1 = (int)c->k2_from_k1q[(size_t)c->k_r2f[kr] * s.nq + qd];
           sg_pairs.gather(c, (size_t)qd * s.ink + kr, 1, Vb, st);
           ++c->launches;
+          // X[t][Q][j][l] = sum_P V[P][j][l] W'[t][P][Q]; W' = conj(W) for TR partners.  Rows are
+          // x = (j, l), columns Q.  V does not depend on tau or spin: it is the shared operand
+          // of the tau batch (sliced once in split precision) and X serves every spin.
+          {
+            ZgemmDesc d;
+            d.M = (int)nn; d.N = N; d.K = N;
+            d.A = Vb; d.a_m.lo = 1; d.a_k = nn;
+            d.B = W; d.b_k = N; d.b_n.lo = 1; d.conjB = trq ? 1 : 0;
+            d.C = SA; d.c_m.lo = 1; d.c_n.lo = nn;
+            d.nb0 = T; d.a_b0 = 0; d.b_b0 = NN; d.c_b0 = Nnn;
+            gemm_main(d, 1);
+          }
           for (int sp = 0; sp < ns; ++sp) {
-            // Y1[t][Q][j][c] = sum_l V[Q][j][l] G^{k1}(tau_t)[l][c]
+            // Z[t][Q][j][c] = sum_l X[t][Q][j][l] G^{k1}(tau_t)[l][c]
             {
               ZgemmDesc d;
               d.M = N * n; d.N = n; d.K = n;
-              d.A = Vb; d.a_m.lo = n; d.a_k = 1;
+              d.A = SA; d.a_m.lo = n; d.a_k = 1;
               d.B = Gf + ((long)k1 * ns + sp) * T * nn; d.b_k = n; d.b_n.lo = 1;
-              d.C = SA; d.c_m.lo = n; d.c_n.lo = 1;
-              d.nb0 = T; d.a_b0 = 0; d.b_b0 = nn; d.c_b0 = Nnn;
+              d.C = SB; d.c_m.lo = n; d.c_n.lo = 1;
+              d.nb0 = T; d.a_b0 = Nnn; d.b_b0 = nn; d.c_b0 = Nnn;
               gemm(d);
             }
-            // Z[t][Q][x] = sum_P Y1[t][P][x] W'[t][P][Q]; W' = conj(W) for TR partners.
-            // Rows are x = (j, c) (the large operand, read once per column tile), columns Q.
-            {
-              ZgemmDesc d;
-              d.M = (int)nn; d.N = N; d.K = N;
-              d.A = SA; d.a_m.lo = 1; d.a_k = nn;
-              d.B = W; d.b_k = N; d.b_n.lo = 1; d.conjB = trq ? 1 : 0;
-              d.C = SB; d.c_m.lo = 1; d.c_n.lo = nn;
-              d.nb0 = T; d.a_b0 = Nnn; d.b_b0 = NN; d.c_b0 = Nnn;
-              gemm_main(d, 1);
-            }
             // Sigma[t][sp][kr][j][i] += -1/nk sum_Q sum_c Z[t][Q][j][c] conj(V[Q][i][c])
+            // (one GEMM over all tau: rows m = (t, j), V is the shared operand)
             {
               ZgemmDesc d;
-              d.M = n; d.N = n; d.K = n; d.KB = N;
-              d.A = SB; d.a_m.lo = n; d.a_k = 1; d.a_kb = nn;
+              d.M = T * n; d.N = n; d.K = n; d.KB = N;
+              d.A = SB; d.a_m.split = n; d.a_m.hi = Nnn; d.a_m.lo = n; d.a_k = 1; d.a_kb = nn;
               d.B = Vb; d.b_k = 1; d.b_n.lo = n; d.b_kb = nn; d.conjB = 1;
-              d.C = Sigma_dev + ((long)sp * s.ink + kr) * nn; d.c_m.lo = n; d.c_n.lo = 1;
-              d.nb0 = T; d.a_b0 = Nnn; d.b_b0 = 0; d.c_b0 = (long)ns * s.ink * nn;
+              d.C = Sigma_dev + ((long)sp * s.ink + kr) * nn;
+              d.c_m.split = n; d.c_m.hi = (long)ns * s.ink * nn; d.c_m.lo = n; d.c_n.lo = 1;
               d.alpha = make_double2(-1.0 / nk, 0.0);
               d.beta = make_double2(1.0, 0.0);
               gemm(d);

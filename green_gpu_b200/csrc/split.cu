@@ -2,20 +2,26 @@
 //
 // Ozaki scheme with exact INT8 slices:
 //   * every row m of A (over the whole reduction K, all K-batches) gets an exponent e_m with
-//     max_k |A(m,k)| < 2^e_m; x = A / 2^e_m is cut into S slices of 7 bits by truncation,
-//     a_s = trunc(2^7 r_{s-1}), r_s = 2^7 r_{s-1} - a_s (all exact in FP64), so
-//     A = 2^e_m sum_s a_s 2^-7s + O(2^(e_m - 7S)).  Columns of B likewise with f_n.
+//     max_k |A(m,k)| < 2^e_m; x = A / 2^e_m is cut into S slices by rounding to nearest,
+//     a_1 = rint(2^6 x), a_s = rint(2^7 r_{s-1}) (|a_s| <= 64, all steps exact in FP64), so
+//     A = 2^(e_m+1) sum_s a_s 2^-7s + O(2^(e_m - 7S)) with an unbiased residual.  Columns of
+//     B likewise with f_n.
 //   * complex arithmetic is one real GEMM of size M x 2N x 2K: A' rows interleave (re, im)
 //     along K, B' rows 2n / 2n+1 hold (re, -im) / (im, re), so C'(m, 2n) = Re C(m,n) and
 //     C'(m, 2n+1) = Im C(m,n).
 //   * the products a_s b_t with s + t = d share the scale 2^-7d and accumulate into one
 //     int32 TMEM accumulator per diagonal d = 2..S+1 (pairs with s + t > S + 1 are dropped,
 //     the usual triangular truncation).  K is processed in chunks small enough that no
-//     int32 sum can overflow (S * Kchunk * 127^2 < 2^31), so every chunk is exact; chunks
-//     are drained to FP64 registers and scaled by 2^(e_m + f_n - 7d).
+//     int32 sum can overflow (S * Kchunk * 64^2 < 2^31), so every chunk is exact; chunks
+//     are drained to FP64 registers and scaled by 2^(e_m + f_n + 2 - 7d).
 //
-// Kernel roles (one CTA per SM, 320 threads): warp 0 issues TMA loads (2D tensor maps,
-// 64-byte swizzle, no multicast) of all S slices of an A and a B K-block into a 3-stage
+// Slice layout in HBM: K-blocked planes, slice[(b * S + s) * nkb + kb][row][64 bytes], so that
+// the rows x 64 bytes box of one K block is one contiguous run (a row-major [row][K] layout
+// makes every box row a separate 64-byte access strided by the whole K length, which for
+// the long reductions of the polarization contraction leaves DRAM pages mostly unused).
+//
+// Kernel roles (one CTA per SM, 320 threads): warp 0 issues TMA loads (3D tensor maps over
+// the planes, 64-byte swizzle, no multicast) of all S slices of an A and a B K-block into a
 // ring; warp 1 owns TMEM and issues tcgen05.mma from one thread; warps 2..9 drain TMEM
 // with tcgen05.ld.  Every mbarrier wait is bounded: on time-out the kernel records an error
 // code, stops issuing work, waits (bounded) for what it already issued and frees TMEM.
@@ -51,8 +57,13 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)_
 __device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count));
 }
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes, uint32_t issue) {
+  asm volatile(
+      "{\n\t.reg .pred q;\n\t"
+      "setp.ne.b32 q, %2, 0;\n\t"
+      "@q mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n\t}" ::"r"(smem_u32(b)),
+      "r"(bytes), "r"(issue)
+      : "memory");
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
@@ -72,6 +83,7 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
 // (abort_on_err = false for the teardown waits that must see in-flight work complete)
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* err, int code,
                                           bool abort_on_err = true) {
+  if (mbar_try(b, parity)) return true;  // fast path: no clock read when the phase is complete
   const long long t0 = clock64();
   int n = 0;
   while (!mbar_try(b, parity)) {
@@ -87,11 +99,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile
   return true;
 }
 
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+// box {64 bytes, rows, 1} at (0, row, plane); the innermost coordinate is always 0.
+// Issued by the lane with issue != 0.
+__device__ __forceinline__ void tma_load_plane(void* dst, const CUtensorMap* map, int row, int plane, uint64_t* bar,
+                                               uint32_t issue) {
   asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          smem_u32(dst)),
-      "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      "{\n\t.reg .pred q;\n\t"
+      "setp.ne.b32 q, %6, 0;\n\t"
+      "@q cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n\t}" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(0), "r"(row), "r"(plane), "r"(smem_u32(bar)), "r"(issue)
       : "memory");
 }
 
@@ -101,34 +118,70 @@ __device__ __forceinline__ uint64_t sw64_desc(const void* p) {
   return a | (1ull << 16) | (32ull << 32) | (1ull << 46) | (4ull << 61);
 }
 
-__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+// The issuing warps run their loops with all 32 lanes (warp-uniform control flow, so the
+// descriptors and coordinates stay warp-uniform values); `issue` (lane 0) predicates the
+// single-thread instructions inside the asm.
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc,
+                                       uint32_t issue) {
   asm volatile(
-      "{\n\t.reg .pred p;\n\t"
+      "{\n\t.reg .pred p, q;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+      "setp.ne.b32 q, %5, 0;\n\t"
+      "@q tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(issue));
 }
-__device__ __forceinline__ void mma_commit(uint64_t* b) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(b))
-               : "memory");
+__device__ __forceinline__ void mma_commit(uint64_t* b, uint32_t issue) {
+  asm volatile(
+      "{\n\t.reg .pred q;\n\t"
+      "setp.ne.b32 q, %1, 0;\n\t"
+      "@q tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}" ::"r"(smem_u32(b)),
+      "r"(issue)
+      : "memory");
 }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
+// TMEM loads without the wait (several loads share one tcgen05.wait::ld); reg_fence makes
+// the loaded registers depend on the wait so no use is scheduled before it
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int* r) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
         "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
-
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, int* r) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
                : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void reg_fence8(int* r) {
+  asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]));
+}
+
+// x * 2^e: one multiply by a constructed power of two while 2^e is a normal number
+__device__ __forceinline__ double scale_pow2(double x, int e) {
+  if (e >= -1022 && e <= 1023) return x * __longlong_as_double((long long)(e + 1023) << 52);
+  return ldexp(x, e);
+}
+
+// drain `NC` int32 columns (a multiple of 8, at most 32) starting at taddr into acc * scale
+template <int NC>
+__device__ __forceinline__ void drain_cols(uint32_t taddr, double* acc, double scale) {
+  int r[32];
+#pragma unroll
+  for (int j = 0; j < NC / 16; ++j) tmem_ld16(taddr + j * 16, r + j * 16);
+  if constexpr (NC % 16 == 8) tmem_ld8(taddr + (NC / 16) * 16, r + (NC / 16) * 16);
+  tmem_wait_ld();
+#pragma unroll
+  for (int j = 0; j < NC / 8; ++j) reg_fence8(r + j * 8);
+#pragma unroll
+  for (int i = 0; i < NC; ++i) {
+    // exact int32 -> double: the bits (0x43380000, r + 2^31) encode 2^52 + 2^51 + r + 2^31
+    const double x = __hiloint2double(0x43380000, r[i] ^ (int)0x80000000) - 6755401588539392.0;
+    acc[i] = fma(x, scale, acc[i]);
+  }
 }
 
 struct I8Args {
@@ -152,6 +205,7 @@ struct I8Args {
   int stages;
   int tmem_cols;
   int nbuf;  // accumulator sets in TMEM (1 or 2)
+  int a_shared, b_shared;  // operand identical for every batch: sliced once, planes / exponents of batch 0
   int* err;
 };
 
@@ -161,42 +215,44 @@ struct Unit {
 };
 
 __device__ __forceinline__ Unit unit_of(const I8Args& p, long u, int BN) {
+  // 32-bit arithmetic: the host keeps units, splits * nkb and the batch count below 2^31
+  const unsigned uu = (unsigned)u;
+  const unsigned ntile = (unsigned)(p.tiles_m * p.tiles_n);
+  const unsigned tile = uu % ntile, rest = uu / ntile;
+  const unsigned spl = (unsigned)p.splits;
   Unit w;
-  const int ntile = p.tiles_m * p.tiles_n;
-  const int tile = (int)(u % ntile);
-  const long rest = u / ntile;
-  w.split = (int)(rest % p.splits);
-  w.batch = rest / p.splits;
-  w.m0 = (tile % p.tiles_m) * BM;
-  w.n0 = (tile / p.tiles_m) * BN;
-  w.kb0 = (int)((long)p.nkb * w.split / p.splits);
-  w.kb1 = (int)((long)p.nkb * (w.split + 1) / p.splits);
+  w.split = (int)(rest % spl);
+  w.batch = (long)(rest / spl);
+  w.m0 = (int)(tile % (unsigned)p.tiles_m) * BM;
+  w.n0 = (int)(tile / (unsigned)p.tiles_m) * BN;
+  w.kb0 = (int)((unsigned)p.nkb * (unsigned)w.split / spl);
+  w.kb1 = (int)((unsigned)p.nkb * (unsigned)(w.split + 1) / spl);
   return w;
-}
-
-__device__ __forceinline__ bool seg_last(const Unit& w, int kb, int kcb) {
-  return (kb + 1 == w.kb1) || ((kb + 1) % kcb == 0);
 }
 
 // Persistent: one CTA per SM walks the work units u = blockIdx.x + i * gridDim.x.  The TMA
 // ring runs on across units; TMEM holds nbuf accumulator sets (S diagonals x BN columns
-// each).  With two sets, consecutive K segments alternate so that draining one overlaps the
-// MMAs of the next; with one set the tile is as wide as 512 / S columns allow, which halves
-// the operand bytes per MAC - the better trade when L2 bandwidth is the limit.
-template <int BN>
+// each).  Every diagonal has its own pair of barriers (MMAs done / drained), so the
+// epilogue drains diagonal d while the MMAs of the later diagonals still run, and the next
+// segment's MMAs into diagonal d start as soon as it is drained: with one set (S >= 3, the
+// tile as wide as 512 / S columns allow) the drain overlaps the next tile's first K block,
+// with two sets (S = 2) consecutive segments alternate.  S is a template parameter so the
+// MMA issue loop unrolls into one tcgen05.mma per instruction slot with precomputed
+// shared-memory descriptors.
+template <int S, int BN>
 __global__ void __launch_bounds__(NTHREADS, 1)
     i8_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, I8Args p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  const int S = p.S;
-  const int stA = S * BM * KB, stB = S * BN * KB;
+  constexpr int stA = S * BM * KB, stB = S * BN * KB;
+  constexpr int ND = 8;  // barrier slots per accumulator set (one per diagonal, S <= 8)
   uint8_t* sA = smem;
   uint8_t* sB = smem + p.stages * stA;
   uint64_t* full = (uint64_t*)(sB + p.stages * stB);
   uint64_t* empty = full + p.stages;
-  uint64_t* accf = empty + p.stages;   // [2]
-  uint64_t* acce = accf + 2;           // [2]
-  uint64_t* fin = acce + 2;
+  uint64_t* accf = empty + p.stages;   // [2][ND]
+  uint64_t* acce = accf + 2 * ND;      // [2][ND]
+  uint64_t* fin = acce + 2 * ND;
   uint32_t* tslot = (uint32_t*)(fin + 1);
   volatile int* err = p.err;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -206,7 +262,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       mbar_init(&full[i], 1);
       mbar_init(&empty[i], 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < 2 * ND; ++b) {
       mbar_init(&accf[b], 1);
       mbar_init(&acce[b], 8);
     }
@@ -222,25 +278,32 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  const uint32_t buf_cols = (uint32_t)(S * BN);
+  constexpr uint32_t buf_cols = (uint32_t)(S * BN);
 
+  const uint32_t leader = lane == 0 ? 1u : 0u;
   if (warp == 0) {
-    // ---------------- TMA producer
-    if (lane == 0) {
+    // ---------------- TMA producer (whole warp, lane 0 issues)
+    {
+      // ring position (stage, phase) kept incrementally: no divisions in the K loop
       long it = 0;
+      int st = 0;
+      uint32_t ph = 0;
       bool ok = true;
       for (long u = blockIdx.x; u < p.units && ok; u += gridDim.x) {
         const Unit w = unit_of(p, u, BN);
-        const int rowA = (int)((w.batch * S) * p.rows_a_pad + w.m0);
-        const int rowB = (int)((w.batch * S) * p.rows_b_pad + w.n0);
+        const int planeA0 = p.a_shared ? 0 : (int)(w.batch * S * p.nkb);
+        const int planeB0 = p.b_shared ? 0 : (int)(w.batch * S * p.nkb);
         for (int kb = w.kb0; kb < w.kb1; ++kb, ++it) {
-          const int st = (int)(it % p.stages);
-          const uint32_t round = (uint32_t)(it / p.stages);
-          if (!mbar_wait(&empty[st], (round & 1) ^ 1, err, 1)) { ok = false; break; }
-          mbar_expect_tx(&full[st], (uint32_t)(stA + stB));
+          if (!__all_sync(0xffffffffu, mbar_wait(&empty[st], ph ^ 1, err, 1))) { ok = false; break; }
+          mbar_expect_tx(&full[st], (uint32_t)(stA + stB), leader);
+#pragma unroll
           for (int s = 0; s < S; ++s) {
-            tma_load_2d(sA + st * stA + s * BM * KB, &tmA, kb * KB, rowA + s * p.rows_a_pad, &full[st]);
-            tma_load_2d(sB + st * stB + s * BN * KB, &tmB, kb * KB, rowB + s * p.rows_b_pad, &full[st]);
+            tma_load_plane(sA + st * stA + s * BM * KB, &tmA, w.m0, planeA0 + s * p.nkb + kb, &full[st], leader);
+            tma_load_plane(sB + st * stB + s * BN * KB, &tmB, w.n0, planeB0 + s * p.nkb + kb, &full[st], leader);
+          }
+          if (++st == p.stages) {
+            st = 0;
+            ph ^= 1;
           }
         }
       }
@@ -250,49 +313,70 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           mbar_wait(&full[j % p.stages], (uint32_t)((j / p.stages) & 1), err, 16, false);
     }
   } else if (warp == 1) {
-    // ---------------- MMA issuer
-    if (lane == 0) {
+    // ---------------- MMA issuer (whole warp, lane 0 issues)
+    {
       const uint32_t idesc =
           (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
-      long it = 0, g = 0;
+      // descriptors of stage 0; a stage / slice / K offset adds (bytes >> 4) to the address
+      // field (all of shared memory stays below 2^18 bytes, so the field never carries)
+      const uint64_t dA0 = sw64_desc(sA), dB0 = sw64_desc(sB);
+      // ring position (st, ph), accumulator set (buf) and its use count (use), and the
+      // position inside the exact-int32 chunk (kin) are all kept incrementally
+      int st = 0, buf = 0;
+      uint32_t ph = 0;
+      long use = 0;
       bool ok = true;
       for (long u = blockIdx.x; u < p.units && ok; u += gridDim.x) {
         const Unit w = unit_of(p, u, BN);
-        for (int kb = w.kb0; kb < w.kb1 && ok; ++kb, ++it) {
-          const int st = (int)(it % p.stages);
-          const uint32_t round = (uint32_t)(it / p.stages);
-          const bool first_in_seg = (kb == w.kb0) || (kb % p.kcb == 0);
-          const int buf = (int)(g % p.nbuf);
-          if (first_in_seg && g >= p.nbuf) {
-            if (!mbar_wait(&acce[buf], (uint32_t)(((g / p.nbuf) - 1) & 1), err, 2)) { ok = false; break; }
-          }
-          if (!mbar_wait(&full[st], round & 1, err, 4)) { ok = false; break; }
+        int kin = w.kb0 % p.kcb;
+        for (int kb = w.kb0; kb < w.kb1 && ok; ++kb) {
+          const bool first = (kb == w.kb0) || kin == 0;
+          const bool last = (kb + 1 == w.kb1) || kin + 1 == p.kcb;
+          const bool reuse = first && use > 0;
+          const uint32_t par_e = (uint32_t)((use - 1) & 1);
+          if (!__all_sync(0xffffffffu, mbar_wait(&full[st], ph, err, 4))) { ok = false; break; }
           tc_fence_after();
-          const uint8_t* a = sA + st * stA;
-          const uint8_t* b = sB + st * stB;
+          const uint64_t da = dA0 + (uint64_t)((st * stA) >> 4);
+          const uint64_t db = dB0 + (uint64_t)((st * stB) >> 4);
+#pragma unroll
           for (int d = 2; d <= S + 1; ++d) {
+            if (reuse) {
+              // diagonal d of this set still holds the previous segment until it is drained
+              if (!__all_sync(0xffffffffu, mbar_wait(&acce[buf * ND + d - 2], par_e, err, 2))) {
+                ok = false;
+                break;
+              }
+              tc_fence_after();
+            }
             const uint32_t tacc = tmem + (uint32_t)buf * buf_cols + (uint32_t)((d - 2) * BN);
             const int s_lo = d - S > 1 ? d - S : 1, s_hi = d - 1 < S ? d - 1 : S;
+#pragma unroll
             for (int s = s_lo; s <= s_hi; ++s) {
               const int t = d - s;
-              const uint64_t da = sw64_desc(a + (s - 1) * BM * KB);
-              const uint64_t db = sw64_desc(b + (t - 1) * BN * KB);
 #pragma unroll
               for (int kk = 0; kk < KB / 32; ++kk) {
-                const uint32_t accum = (first_in_seg && s == s_lo && kk == 0) ? 0u : 1u;
-                mma_i8(tacc, da + (uint64_t)(kk * 2), db + (uint64_t)(kk * 2), idesc, accum);
+                const uint32_t accum = (first && s == s_lo && kk == 0) ? 0u : 1u;
+                mma_i8(tacc, da + (uint64_t)(((s - 1) * BM * KB) >> 4) + (uint64_t)(kk * 2),
+                       db + (uint64_t)(((t - 1) * BN * KB) >> 4) + (uint64_t)(kk * 2), idesc, accum, leader);
               }
             }
+            if (last) mma_commit(&accf[buf * ND + d - 2], leader);
           }
-          mma_commit(&empty[st]);
-          if (seg_last(w, kb, p.kcb)) {
-            mma_commit(&accf[buf]);
-            ++g;
+          if (!ok) break;
+          mma_commit(&empty[st], leader);
+          if (++st == p.stages) {
+            st = 0;
+            ph ^= 1;
+          }
+          if (++kin == p.kcb) kin = 0;
+          if (last && ++buf == p.nbuf) {
+            buf = 0;
+            ++use;
           }
         }
       }
-      // all MMAs issued by this thread complete before TMEM can be freed
-      mma_commit(fin);
+      // all MMAs issued by lane 0 complete before TMEM can be freed
+      mma_commit(fin, leader);
       mbar_wait(fin, 0, err, 32, false);
     }
   } else {
@@ -301,65 +385,75 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const int row = q * 32 + lane;
     constexpr int HC = BN / 2;  // int32 columns per thread
     double acc[HC];
-    long g = 0;
+    int buf = 0;
+    uint32_t par = 0;
     bool ok = true;
     for (long u = blockIdx.x; u < p.units && ok; u += gridDim.x) {
       const Unit w = unit_of(p, u, BN);
+      // exponents of this tile, loaded before the drain so that their latency overlaps it:
+      // the row exponent per thread (padded rows carry exponent 0), the column exponents of
+      // this half-tile one per lane, broadcast by shuffles in the output loop
+      const int m = w.m0 + row;
+      const int ea = p.ea[(p.a_shared ? 0 : w.batch) * p.rows_a_pad + m];
+      const int nbase = (w.n0 + h * HC) / 2;
+      const long ebo = (p.b_shared ? 0 : w.batch) * (long)p.N;
+      const int eb_lane = (lane < HC / 2 && nbase + lane < p.N) ? p.eb[ebo + nbase + lane] : 0;
 #pragma unroll
       for (int i = 0; i < HC; ++i) acc[i] = 0.0;
-      for (int kb = w.kb0; kb < w.kb1; ++kb) {
-        if (!seg_last(w, kb, p.kcb)) continue;
-        const int buf = (int)(g % p.nbuf);
-        if (!mbar_wait(&accf[buf], (uint32_t)((g / p.nbuf) & 1), err, 8)) { ok = false; break; }
-        tc_fence_after();
+      // one drain per K segment: segments end at kb1 and at every multiple of kcb
+      for (int k0 = w.kb0; k0 < w.kb1 && ok; k0 = min(w.kb1, (k0 / p.kcb + 1) * p.kcb)) {
+#pragma unroll
         for (int d = 2; d <= S + 1; ++d) {
-          const double scale = ldexp(1.0, -7 * d);
+          if (!mbar_wait(&accf[buf * ND + d - 2], par, err, 8)) { ok = false; break; }
+          tc_fence_after();
+          const double scale = __longlong_as_double((long long)(1023 - 7 * d) << 52);  // 2^-7d
           const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)buf * buf_cols +
                                 (uint32_t)((d - 2) * BN + h * HC);
+          // groups of 32 columns, one wait per group
 #pragma unroll
-          for (int j = 0; j < HC / 16; ++j) {
-            int r[16];
-            tmem_ld16(base + j * 16, r);
+          for (int j = 0; j < HC / 32; ++j) drain_cols<32>(base + j * 32, acc + j * 32, scale);
+          if constexpr (HC % 32 != 0) drain_cols<HC % 32>(base + (HC / 32) * 32, acc + (HC / 32) * 32, scale);
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acce[buf * ND + d - 2]);
+        }
+        if (++buf == p.nbuf) {
+          buf = 0;
+          par ^= 1;
+        }
+      }
+      if (!ok) break;
+      // output: consecutive lanes hold consecutive rows m, so every store instruction is
+      // coalesced wherever C (or the split-K workspace, [split][batch][n][m]) is m-contiguous
+      const int b0 = (int)(w.batch % p.nb0);
+      const int b1 = (int)((w.batch / p.nb0) % p.nb1);
+      const int b2 = (int)(w.batch / ((long)p.nb0 * p.nb1));
+      const bool use_beta = p.beta.x != 0.0 || p.beta.y != 0.0;
+      const bool mok = m < p.M;
+      double2* crow = p.C + b0 * p.c_b0 + b1 * p.c_b1 + b2 * p.c_b2 + (mok ? p.c_m(m) : 0);
+      double2* wrow = p.work + (w.split * p.batch + w.batch) * (long)p.N * p.M + m;
+      // column offset c_n(n) stepped through the tile: (nq, nr) = divmod(n, split)
+      const int csp = p.c_n.split > 0 ? p.c_n.split : 1 << 30;
+      int nq = nbase / csp, nr = nbase - nq * csp;
 #pragma unroll
-            for (int i = 0; i < 16; ++i) acc[j * 16 + i] += (double)r[i] * scale;
-          }
-          if constexpr (HC % 16 == 8) {
-            // BN = 48 / 80: the last 8 columns of the half
-            int r[8];
-            tmem_ld8(base + (HC / 16) * 16, r);
-#pragma unroll
-            for (int i = 0; i < 8; ++i) acc[(HC / 16) * 16 + i] += (double)r[i] * scale;
+      for (int c = 0; c < HC / 2; ++c) {
+        const int eb = __shfl_sync(0xffffffffu, eb_lane, c);
+        const int n = nbase + c;
+        if (mok && n < p.N) {
+          const int e = ea + eb + 2;  // x = 2 sum d_s 2^-7s per operand
+          const double2 v = make_double2(scale_pow2(acc[2 * c], e), scale_pow2(acc[2 * c + 1], e));
+          if (p.splits > 1) {
+            wrow[(long)n * p.M] = v;
+          } else {
+            double2* cp = crow + (p.c_n.split > 0 ? nq * p.c_n.hi + nr * p.c_n.lo : (long)n * p.c_n.lo);
+            double2 o = cmul(p.alpha, v);
+            if (use_beta) o = cadd(o, cmul(p.beta, *cp));
+            *cp = o;
           }
         }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&acce[buf]);
-        ++g;
-      }
-      if (!ok || *err) break;
-      const int m = w.m0 + row;
-      if (m < p.M) {
-        const int ea = p.ea[w.batch * p.rows_a_pad + m];
-        const int b0 = (int)(w.batch % p.nb0);
-        const int b1 = (int)((w.batch / p.nb0) % p.nb1);
-        const int b2 = (int)(w.batch / ((long)p.nb0 * p.nb1));
-        const bool use_beta = p.beta.x != 0.0 || p.beta.y != 0.0;
-        const int nbase = (w.n0 + h * HC) / 2;
-#pragma unroll
-        for (int c = 0; c < HC / 2; ++c) {
-          const int n = nbase + c;
-          if (n < p.N) {
-            const int e = ea + __ldg(&p.eb[w.batch * p.N + n]);
-            const double2 v = make_double2(ldexp(acc[2 * c], e), ldexp(acc[2 * c + 1], e));
-            if (p.splits > 1) {
-              p.work[((w.split * p.batch + w.batch) * p.M + m) * (long)p.N + n] = v;
-            } else {
-              double2* cp = p.C + b0 * p.c_b0 + b1 * p.c_b1 + b2 * p.c_b2 + p.c_m(m) + p.c_n(n);
-              double2 o = cmul(p.alpha, v);
-              if (use_beta) o = cadd(o, cmul(p.beta, *cp));
-              *cp = o;
-            }
-          }
+        if (++nr == csp) {
+          nr = 0;
+          ++nq;
         }
       }
     }
@@ -388,6 +482,15 @@ struct OpView {
   }
 };
 
+// IdxMap with 32-bit index arithmetic (every row and K index of an operand is below 2^31)
+__device__ __forceinline__ long map32(const IdxMap& m, int i) {
+  if (m.split > 0) {
+    const int q = i / m.split;
+    return (long)q * m.hi + (long)(i - q * m.split) * m.lo;
+  }
+  return (long)i * m.lo;
+}
+
 // exponent per (batch, row): e with max |x| < 2^e over all (kb, k); one warp per row
 __global__ void row_exponent_kernel(OpView v, int rows_pad, int* out, long nbatch) {
   const long gw = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
@@ -398,12 +501,19 @@ __global__ void row_exponent_kernel(OpView v, int rows_pad, int* out, long nbatc
   const int r = (int)(gw % rows_pad);
   double mx = 0.0;
   if (r < v.R) {
-    const double2* base = v.ptr(b) + v.rmap(r);
-    const long n = (long)v.KB * v.K;
-    for (long i = lane; i < n; i += 32) {
-      const long kb = i / v.K, k = i % v.K;
-      const double2 x = base[kb * v.kbs + k * v.ks];
+    const double2* base = v.ptr(b) + map32(v.rmap, r);
+    // (kb, k) stepped without divisions: lane i starts at i and advances by 32
+    int kb = lane / v.K, k = lane - kb * v.K;
+    const int step_kb = 32 / v.K, step_k = 32 - step_kb * v.K;
+    for (; kb < v.KB; ) {
+      const double2 x = base[(long)kb * v.kbs + (long)k * v.ks];
       mx = fmax(mx, fmax(fabs(x.x), fabs(x.y)));
+      kb += step_kb;
+      k += step_k;
+      if (k >= v.K) {
+        k -= v.K;
+        ++kb;
+      }
     }
   }
   for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -419,7 +529,7 @@ __global__ void row_exponent_rc_kernel(OpView v, int rows_pad, int* out, long nb
   const int r = (int)(gt % rows_pad);
   double mx = 0.0;
   if (r < v.R) {
-    const double2* base = v.ptr(b) + v.rmap(r);
+    const double2* base = v.ptr(b) + map32(v.rmap, r);
     for (int kb = 0; kb < v.KB; ++kb)
       for (int k = 0; k < v.K; ++k) {
         const double2 x = base[kb * v.kbs + (long)k * v.ks];
@@ -429,67 +539,102 @@ __global__ void row_exponent_rc_kernel(OpView v, int rows_pad, int* out, long nb
   out[gt] = mx > 0.0 ? ilogb(mx) + 1 : 0;
 }
 
-// cut x (|x| < 1 after scaling) into S int8 slices by truncation
-__device__ __forceinline__ void cut(double x, int S, int8_t* d) {
+// cut x (|x| < 1 after scaling) into S int8 slices by rounding to nearest:
+// d_1 = rint(64 x), r_1 = 64 x - d_1 in [-1/2, 1/2]; d_s = rint(128 r_{s-1}), ...
+// so x = 2 sum_s d_s 2^-7s + O(2^-7S), every |d_s| <= 64 and the residual is unbiased.
+// rint is done by adding 2^52 + 2^51 (the sum is rounded to an integer, round-to-nearest-
+// even like rint, and its low word holds that integer in two's complement); every step is
+// exact in FP64 and uses only the add / fma pipes.
+template <int S>
+__device__ __forceinline__ void cut(double x, int8_t* d) {
+  const double RND = 6755399441055744.0;  // 2^52 + 2^51
+  x *= 64.0;
+#pragma unroll
   for (int s = 0; s < S; ++s) {
-    x *= 128.0;
-    const double t = trunc(x);
-    d[s] = (int8_t)t;
-    x -= t;
+    const double y = x + RND;
+    d[s] = (int8_t)__double2loint(y);
+    const double t = y - RND;
+    x = (x - t) * 128.0;
   }
 }
 
-// Slices of a row operand (A side): out[((b*S + s)*rows_pad + r)*kp + 2*kk + {0,1}].
-// A 32 x 32 (row, kk) tile goes through shared memory so global reads follow the
-// operand's contiguous direction (rows or k) and writes are along k.
-template <bool BSIDE>
-__global__ void slice_kernel(OpView v, int S, int rows_pad, long kp, const int* ex, int8_t* out, long nbatch) {
+// x * 2^-e, exact while the result is a normal number (ldexp outside the directly encodable range)
+__device__ __forceinline__ double scale_neg(double x, int e) {
+  if (e > -1000 && e < 1000) return x * __longlong_as_double((long long)(1023 - e) << 52);
+  return ldexp(x, -e);
+}
+
+// Slices of a row operand (A side): out[(((b*S + s)*nkb + kb)*rows_pad + r)*64 + 2*kk' + {0,1}]
+// with kk = 32 kb + kk' (one 32-complex k tile is one 64-byte K block).  A 32 x 32 (row, kk)
+// tile goes through shared memory so global reads follow the operand's contiguous direction
+// (rows or k) and each warp writes 64 contiguous bytes.
+template <bool BSIDE, int S>
+__global__ void slice_kernel(OpView v, int rows_pad, int ktiles, const int* ex, int8_t* out, long nbatch) {
   __shared__ double2 tile[32][33];
-  const long Ktot = (long)v.KB * v.K;
-  const long ktiles = (kp / 2 + 31) / 32;
-  const long rtiles = rows_pad / 32;
+  const int Ktot = v.KB * v.K;
+  const int rtiles = rows_pad / 32;
   long t = blockIdx.x;
-  const long kt = t % ktiles;
+  const int kt = (int)(t % ktiles);
   t /= ktiles;
-  const long rt = t % rtiles;
+  const int rt = (int)(t % rtiles);
   const long b = t / rtiles;
   if (b >= nbatch) return;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
   const double2* base = v.ptr(b);
-  const bool rcontig = (v.rmap.split == 0 && v.rmap.lo == 1) || (v.rmap.split > 0 && v.rmap.lo == 1);
+  const bool rcontig = v.rmap.lo == 1;
   // load: tile[rr][kk]
-  for (int i = ty; i < 32; i += 8) {
-    int rr, kk;
-    if (rcontig) { rr = tx; kk = i; } else { rr = i; kk = tx; }
-    const long r = rt * 32 + rr, k = kt * 32 + kk;
-    double2 x = make_double2(0.0, 0.0);
-    if (r < v.R && k < Ktot) {
-      const long kbi = k / v.K, ki = k % v.K;
-      x = base[v.rmap(r) + kbi * v.kbs + ki * v.ks];
-      if (v.conj) x.y = -x.y;
+  if (rcontig) {
+    // rr = tx (fixed row per thread), kk = i
+    const int r = rt * 32 + tx;
+    const bool rok = r < v.R;
+    const double2* rowp = base + (rok ? map32(v.rmap, r) : 0);
+    for (int i = ty; i < 32; i += 8) {
+      const int k = kt * 32 + i;
+      double2 x = make_double2(0.0, 0.0);
+      if (rok && k < Ktot) {
+        const int kbi = k / v.K, ki = k - kbi * v.K;
+        x = rowp[kbi * v.kbs + (long)ki * v.ks];
+        if (v.conj) x.y = -x.y;
+      }
+      tile[tx][i] = x;
     }
-    tile[rr][kk] = x;
+  } else {
+    // kk = tx (fixed k per thread), rr = i
+    const int k = kt * 32 + tx;
+    const bool kok = k < Ktot;
+    const int kbi = kok ? k / v.K : 0, ki = kok ? k - kbi * v.K : 0;
+    const long koff = kbi * v.kbs + (long)ki * v.ks;
+    for (int i = ty; i < 32; i += 8) {
+      const int r = rt * 32 + i;
+      double2 x = make_double2(0.0, 0.0);
+      if (kok && r < v.R) {
+        x = base[map32(v.rmap, r) + koff];
+        if (v.conj) x.y = -x.y;
+      }
+      tile[i][tx] = x;
+    }
   }
   __syncthreads();
   // write: thread (ty -> row, tx -> kk)
   for (int i = ty; i < 32; i += 8) {
-    const long r = rt * 32 + i, kk = kt * 32 + tx;
-    if (r >= rows_pad || 2 * kk >= kp) continue;
+    const int r = rt * 32 + i;
     const double2 x = tile[i][tx];
     const int e = (r < v.R) ? ex[b * (BSIDE ? v.R : rows_pad) + r] : 0;
-    int8_t dr[8], di[8];
-    cut(ldexp(x.x, -e), S, dr);
-    cut(ldexp(x.y, -e), S, di);
+    int8_t dr[S], di[S];
+    cut<S>(scale_neg(x.x, e), dr);
+    cut<S>(scale_neg(x.y, e), di);
     if (!BSIDE) {
+#pragma unroll
       for (int s = 0; s < S; ++s) {
-        int8_t* o = out + (((b * S + s) * rows_pad + r) * kp + 2 * kk);
+        int8_t* o = out + ((((b * S + s) * ktiles + kt) * rows_pad + r) * KB + 2 * tx);
         *(char2*)o = make_char2(dr[s], di[s]);
       }
     } else {
       // B' rows 2r: (re, -im); 2r + 1: (im, re); rows_pad here counts complex columns
+#pragma unroll
       for (int s = 0; s < S; ++s) {
-        int8_t* o0 = out + (((b * S + s) * (2L * rows_pad) + 2 * r) * kp + 2 * kk);
-        int8_t* o1 = o0 + kp;
+        int8_t* o0 = out + ((((b * S + s) * ktiles + kt) * (2L * rows_pad) + 2 * r) * KB + 2 * tx);
+        int8_t* o1 = o0 + KB;
         *(char2*)o0 = make_char2(dr[s], (int8_t)(-di[s]));
         *(char2*)o1 = make_char2(di[s], dr[s]);
       }
@@ -504,10 +649,10 @@ __global__ void split_reduce_kernel(const double2* work, int splits, long batch_
   const long total = batch_count * mn;
   const bool use_beta = beta.x != 0.0 || beta.y != 0.0;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-    const long b = i / mn, e = i % mn;
+    const long b = i / mn, e = i % mn;  // e = n * M + m (the workspace is m-contiguous)
     double2 acc = make_double2(0.0, 0.0);
     for (int s = 0; s < splits; ++s) acc = cadd(acc, work[(s * batch_count + b) * mn + e]);
-    const int m = (int)(e / N), n = (int)(e % N);
+    const int n = (int)(e / M), m = (int)(e % M);
     const int b0 = (int)(b % nb0), b1 = (int)((b / nb0) % nb1), b2 = (int)(b / ((long)nb0 * nb1));
     double2* cp = C + b0 * c_b0 + b1 * c_b1 + b2 * c_b2 + c_m(m) + c_n(n);
     double2 o = cmul(alpha, acc);
@@ -535,14 +680,16 @@ EncodeTiled encode_fn() {
   return fn;
 }
 
-CUtensorMap make_map(const int8_t* base, long kp, long rows, int box_rows) {
+// planes of rows_pad x 64 bytes; box = one K block of box_rows rows
+CUtensorMap make_map(const int8_t* base, long rows_pad, long planes, int box_rows) {
+  if (planes > 0x7fffffffL) throw Error(GG_ERR_ARG, "split: too many K-block planes for a tensor map");
   CUtensorMap m;
   std::memset(&m, 0, sizeof(m));
-  const cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)kp};
-  const cuuint32_t box[2] = {(cuuint32_t)KB, (cuuint32_t)box_rows};
-  const cuuint32_t estr[2] = {1, 1};
-  CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)base, dims, strides, box, estr,
+  const cuuint64_t dims[3] = {(cuuint64_t)KB, (cuuint64_t)rows_pad, (cuuint64_t)planes};
+  const cuuint64_t strides[2] = {(cuuint64_t)KB, (cuuint64_t)(rows_pad * KB)};
+  const cuuint32_t box[3] = {(cuuint32_t)KB, (cuuint32_t)box_rows, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void*)base, dims, strides, box, estr,
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw Error(GG_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
@@ -559,16 +706,40 @@ int sms() {
   return n;
 }
 
-template <int BN>
+template <int S, int BN>
 void launch_i8(const CUtensorMap& ta, const CUtensorMap& tb, const I8Args& a, long blocks, size_t smem,
                cudaStream_t st) {
   static bool cfg = false;
   if (!cfg) {
-    GG_CUDA(cudaFuncSetAttribute(i8_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448));
+    GG_CUDA(cudaFuncSetAttribute(i8_gemm_kernel<S, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448));
     cfg = true;
   }
-  i8_gemm_kernel<BN><<<(unsigned)blocks, NTHREADS, smem, st>>>(ta, tb, a);
+  i8_gemm_kernel<S, BN><<<(unsigned)blocks, NTHREADS, smem, st>>>(ta, tb, a);
   GG_CHECK_LAUNCH();
+}
+
+template <int S>
+void launch_slices_s(const OpView& va, const OpView& vb, int rows_a_pad, int ncol_pad, int nkb, const int* ea,
+                     const int* eb, int8_t* a8, int8_t* b8, long batch_a, long batch_b, cudaStream_t st) {
+  slice_kernel<false, S><<<(unsigned)((long)nkb * (rows_a_pad / 32) * batch_a), 256, 0, st>>>(va, rows_a_pad, nkb, ea,
+                                                                                             a8, batch_a);
+  GG_CHECK_LAUNCH();
+  slice_kernel<true, S><<<(unsigned)((long)nkb * (ncol_pad / 32) * batch_b), 256, 0, st>>>(vb, ncol_pad, nkb, eb, b8,
+                                                                                          batch_b);
+  GG_CHECK_LAUNCH();
+}
+
+void launch_slices(int S, const OpView& va, const OpView& vb, int rows_a_pad, int ncol_pad, int nkb, const int* ea,
+                   const int* eb, int8_t* a8, int8_t* b8, long batch_a, long batch_b, cudaStream_t st) {
+  switch (S) {
+    case 2: launch_slices_s<2>(va, vb, rows_a_pad, ncol_pad, nkb, ea, eb, a8, b8, batch_a, batch_b, st); break;
+    case 3: launch_slices_s<3>(va, vb, rows_a_pad, ncol_pad, nkb, ea, eb, a8, b8, batch_a, batch_b, st); break;
+    case 4: launch_slices_s<4>(va, vb, rows_a_pad, ncol_pad, nkb, ea, eb, a8, b8, batch_a, batch_b, st); break;
+    case 5: launch_slices_s<5>(va, vb, rows_a_pad, ncol_pad, nkb, ea, eb, a8, b8, batch_a, batch_b, st); break;
+    case 6: launch_slices_s<6>(va, vb, rows_a_pad, ncol_pad, nkb, ea, eb, a8, b8, batch_a, batch_b, st); break;
+    case 7: launch_slices_s<7>(va, vb, rows_a_pad, ncol_pad, nkb, ea, eb, a8, b8, batch_a, batch_b, st); break;
+    default: launch_slices_s<8>(va, vb, rows_a_pad, ncol_pad, nkb, ea, eb, a8, b8, batch_a, batch_b, st); break;
+  }
 }
 
 }  // namespace
@@ -593,20 +764,26 @@ int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
   const int bn_pad = BN * 64 / std::__gcd(BN, 64);  // keeps rows_b_pad / 2 a multiple of 32
   const long batch = (long)d.nb0 * d.nb1 * d.nb2;
   const long Ktot = (long)d.KB * d.K;
+  if (2 * Ktot + KB >= (1L << 31) || (long)d.M >= (1L << 31) || (long)d.N >= (1L << 30))
+    throw Error(GG_ERR_ARG, "split: operand dimensions too large for one launch");
   const long kp = ((2 * Ktot + KB - 1) / KB) * KB;
   const int rows_a_pad = ((d.M + BM - 1) / BM) * BM;
   const int np = 2 * d.N;
   const int rows_b_pad = ((np + bn_pad - 1) / bn_pad) * bn_pad;  // B' rows (2 per complex column)
   const int ncol_pad = rows_b_pad / 2;                // complex columns incl. padding
-  // exact int32 chunk: S * Kchunk * 127^2 < 2^31
-  const long kchunk = std::max<long>(KB, ((2147483647L / (16129L * S)) / KB) * KB);
+  // exact int32 chunk: S * Kchunk * 64^2 < 2^31 (slices are rounded, |d| <= 64)
+  const long kchunk = std::max<long>(KB, ((2147483647L / (4096L * S)) / KB) * KB);
   const int kcb = (int)(kchunk / KB);
   const int nkb = (int)(kp / KB);
 
-  int8_t* a8 = e->a8.ensure((size_t)batch * S * rows_a_pad * kp);
-  int8_t* b8 = e->b8.ensure((size_t)batch * S * rows_b_pad * kp);
-  int* ea = e->ea.ensure((size_t)batch * rows_a_pad);
-  int* eb = e->eb.ensure((size_t)batch * d.N);
+  // an operand with zero batch strides is the same matrix for every batch: slice it once
+  const bool a_shared = batch > 1 && d.a_b0 == 0 && d.a_b1 == 0 && d.a_b2 == 0;
+  const bool b_shared = batch > 1 && d.b_b0 == 0 && d.b_b1 == 0 && d.b_b2 == 0;
+  const long batch_a = a_shared ? 1 : batch, batch_b = b_shared ? 1 : batch;
+  int8_t* a8 = e->a8.ensure((size_t)batch_a * S * rows_a_pad * kp);
+  int8_t* b8 = e->b8.ensure((size_t)batch_b * S * rows_b_pad * kp);
+  int* ea = e->ea.ensure((size_t)batch_a * rows_a_pad);
+  int* eb = e->eb.ensure((size_t)batch_b * d.N);
   int* err = e->err.p;
   if (!err) {
     err = e->err.ensure(1);
@@ -617,28 +794,22 @@ int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
   OpView vb{d.B, d.b_n, d.b_kb, d.b_k, d.KB, d.K, d.N, d.nb0, d.nb1, d.b_b0, d.b_b1, d.b_b2, d.conjB};
   int launches = 0;
   {
-    auto exponents = [&](const OpView& v, int rows_pad, int* out) {
+    auto exponents = [&](const OpView& v, int rows_pad, int* out, long nb) {
       const bool rcontig = v.rmap.lo == 1 && v.ks != 1;
-      const long n = batch * rows_pad;
+      const long n = nb * rows_pad;
       if (rcontig)
-        row_exponent_rc_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(v, rows_pad, out, batch);
+        row_exponent_rc_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(v, rows_pad, out, nb);
       else
-        row_exponent_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(v, rows_pad, out, batch);
+        row_exponent_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(v, rows_pad, out, nb);
       GG_CHECK_LAUNCH();
     };
-    exponents(va, rows_a_pad, ea);
-    exponents(vb, d.N, eb);
-    const long ktiles = (kp / 2 + 31) / 32;
-    slice_kernel<false><<<(unsigned)(ktiles * (rows_a_pad / 32) * batch), 256, 0, st>>>(va, S, rows_a_pad, kp, ea, a8,
-                                                                                        batch);
-    GG_CHECK_LAUNCH();
-    slice_kernel<true><<<(unsigned)(ktiles * (ncol_pad / 32) * batch), 256, 0, st>>>(vb, S, ncol_pad, kp, eb, b8,
-                                                                                    batch);
-    GG_CHECK_LAUNCH();
+    exponents(va, rows_a_pad, ea, batch_a);
+    exponents(vb, d.N, eb, batch_b);
+    launch_slices(S, va, vb, rows_a_pad, ncol_pad, nkb, ea, eb, a8, b8, batch_a, batch_b, st);
     launches += 4;
   }
-  const CUtensorMap ta = make_map(a8, kp, (long)batch * S * rows_a_pad, BM);
-  const CUtensorMap tb = make_map(b8, kp, (long)batch * S * rows_b_pad, BN);
+  const CUtensorMap ta = make_map(a8, rows_a_pad, batch_a * S * nkb, BM);
+  const CUtensorMap tb = make_map(b8, rows_b_pad, batch_b * S * nkb, BN);
 
   I8Args a{};
   a.S = S;
@@ -665,12 +836,14 @@ int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
   a.beta = d.beta;
   a.err = err;
   a.nbuf = nbuf;
+  a.a_shared = a_shared ? 1 : 0;
+  a.b_shared = b_shared ? 1 : 0;
   a.tmem_cols = 32;
   while (a.tmem_cols < nbuf * S * BN) a.tmem_cols *= 2;
   const size_t stage_bytes = (size_t)S * (BM + BN) * KB;
   a.stages = (int)std::min<size_t>(4, (220 * 1024 - 2048) / stage_bytes);
   if (a.stages < 2) throw Error(GG_ERR_ARG, "split: stage does not fit shared memory");
-  const size_t smem = a.stages * stage_bytes + 1024 + 256;
+  const size_t smem = a.stages * stage_bytes + 1024 + 512;  // + alignment + barriers and TMEM slot
   const long base = (long)a.tiles_m * a.tiles_n * batch;
   // split-K so that the units fill whole waves of persistent CTAs (each split keeps >= 8 K blocks)
   int splits = 1;
@@ -696,12 +869,17 @@ int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
   a.splits = splits;
   a.work = e->work.p;
   a.units = base * splits;
+  if (a.units >= (1L << 31) || (long)splits * nkb >= (1L << 31))
+    throw Error(GG_ERR_ARG, "split: too many work units for one launch");
   const long grid = std::min<long>(a.units, sms());
-  switch (BN) {
-    case 128: launch_i8<128>(ta, tb, a, grid, smem, st); break;
-    case 96: launch_i8<96>(ta, tb, a, grid, smem, st); break;
-    case 80: launch_i8<80>(ta, tb, a, grid, smem, st); break;
-    default: launch_i8<64>(ta, tb, a, grid, smem, st); break;
+  switch (S) {  // BN as chosen above for each slice count
+    case 2: launch_i8<2, 128>(ta, tb, a, grid, smem, st); break;
+    case 3: launch_i8<3, 128>(ta, tb, a, grid, smem, st); break;
+    case 4: launch_i8<4, 128>(ta, tb, a, grid, smem, st); break;
+    case 5: launch_i8<5, 96>(ta, tb, a, grid, smem, st); break;
+    case 6: launch_i8<6, 80>(ta, tb, a, grid, smem, st); break;
+    case 7: launch_i8<7, 64>(ta, tb, a, grid, smem, st); break;
+    default: launch_i8<8, 64>(ta, tb, a, grid, smem, st); break;
   }
   ++launches;
   if (splits > 1) {

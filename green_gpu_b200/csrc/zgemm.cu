@@ -250,15 +250,25 @@ int zgemm(const ZgemmDesc& d0, cudaStream_t stream) {
   const int tiles_m = ceil_div(d.M, BM), tiles_n = ceil_div(d.N, BN);
   const long batch = (long)d.nb0 * d.nb1 * d.nb2;
   const long base = (long)tiles_m * tiles_n * batch;
-  // split-K when the grid under-fills the device and the reduction is long
+  // split-K when the grid leaves resident CTA slots idle and the reduction is long: the
+  // split count minimises the waves per unit of work, ceil(base * s / slots) / s (two CTAs
+  // per SM are resident), so a grid of 1.3 waves becomes one of 3 full waves at s = 3
+  // rather than 2.6 waves at s = 2; ties go to the smaller count
   int splits = 1;
   const long ksteps = (long)d.KB * ceil_div(d.K, BK);
-  const long target = 2L * sm_count();
-  if (d.work && base < target && ksteps >= 32) {
-    splits = (int)std::min<long>((target + base - 1) / base, ksteps / 16);
+  const long slots = 2L * sm_count();
+  if (d.work && base < 8 * slots && ksteps >= 32) {
     const long need = (long)d.M * d.N * batch;
-    if (need > 0) splits = (int)std::min<long>(splits, d.work_elems / need);
-    splits = std::max(1, std::min(splits, 64));
+    long smax = std::min<long>(64, ksteps / 16);
+    if (need > 0) smax = std::min<long>(smax, d.work_elems / need);
+    double best = (double)ceil_div(base, slots);
+    for (long s = 2; s <= smax; ++s) {
+      const double cost = (double)((base * s + slots - 1) / slots) / (double)s;
+      if (cost < best * 0.97) {
+        best = cost;
+        splits = (int)s;
+      }
+    }
   }
   d.splits = splits;
   const long blocks = base * splits;

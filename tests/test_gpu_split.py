@@ -52,10 +52,10 @@ def test_fp64_zgemm_matches_numpy(ctx):
 
 
 def test_split_zgemm_exact_for_small_integers(ctx):
-    # integers below 2^6 are represented exactly by the first slice: the result is exact
+    # integers below 2^5 are represented exactly by the first slice: the result is exact
     rng = np.random.default_rng(3)
-    A = rng.integers(-60, 60, (200, 500)) + 1j * rng.integers(-60, 60, (200, 500))
-    B = rng.integers(-60, 60, (500, 150)) + 1j * rng.integers(-60, 60, (500, 150))
+    A = rng.integers(-30, 30, (200, 500)) + 1j * rng.integers(-30, 30, (200, 500))
+    B = rng.integers(-30, 30, (500, 150)) + 1j * rng.integers(-30, 30, (500, 150))
     ctx.set_split_slices(2)
     out = ctx.zgemm(A.astype(np.complex128), B.astype(np.complex128), precision=native.PREC_SPLIT)
     assert np.array_equal(out, (A @ B).astype(np.complex128))
