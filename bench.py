@@ -258,7 +258,7 @@ def main():
     e1 = torch.cuda.Event(enable_timing=True)
     lat = []
     launches = 0
-    kstats = {0: [0, 0.0, 0.0], 1: [0, 0.0, 0.0]}
+    kstats = {w: [0, 0.0, 0.0] for w in (0, 1, 2)}
     with ClockSampler(local) as clk:
         e0.record(stream)
         for _ in range(args.steps):
@@ -270,7 +270,7 @@ def main():
             b.synchronize()
             lat.append(a.elapsed_time(b) * 1e-3)
             launches += ctx.launch_count()
-            for w in (0, 1):
+            for w in (0, 1, 2):
                 st = ctx.kernel_stats(w)
                 kstats[w][0] += st["launches"]
                 kstats[w][1] += st["seconds"]
@@ -297,11 +297,11 @@ def main():
 
     # roofline of the dominant contraction (largest device time)
     pk, pk_src = peaks()
-    dom = max((0, 1), key=lambda w: kstats[w][1])
+    dom = max((0, 1, 2), key=lambda w: kstats[w][1])
     n_l, sec, fl = kstats[dom]
     achieved = fl / sec / 1e12 if sec > 0 else 0.0
     fp64_peak = float(os.environ.get("GG_FP64_PEAK_TFLOPS", "40.0"))
-    kname = "p0_contraction" if dom == 0 else "sigma_contraction"
+    kname = ("p0_contraction", "sigma_contraction", "sigma_final_contraction")[dom]
     if args.precision == "fp64":
         peak, peak_note = fp64_peak, "nominal FP64 tensor (DMMA) peak of B200; no measured FP64 figure"
         unit = "TFLOP/s"
@@ -322,7 +322,9 @@ def main():
         with open(traffic_file) as f:
             tr = json.load(f).get(f"{roof['kernel']}_{args.precision}_{args.config}")
         if tr:
-            roof["traffic"] = tr
+            roof["traffic"] = tr["bytes_per_launch"]
+            roof["traffic_unit"] = "bytes per launch (DRAM read + write, ncu)"
+            roof["traffic_note"] = tr["note"]
 
     flops_build = gw_flop_model(s.nk, s.ink, s.inq, s.ns, s.nts, s.nw_b, s.nao, s.NQ)
     line = {

@@ -353,7 +353,7 @@ int gg_set_profiling(gg_context* c, int enable) {
 }
 
 int gg_kernel_stats(const gg_context* c, int which, int64_t* launches, double* seconds, double* flops) {
-  if (!c || which < 0 || which > 1) return GG_ERR_ARG;
+  if (!c || which < 0 || which > 2) return GG_ERR_ARG;
   if (launches) *launches = c->kstat_launches[which];
   if (seconds) *seconds = c->kstat_seconds[which];
   if (flops) *flops = c->kstat_flops[which];

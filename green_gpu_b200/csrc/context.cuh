@@ -99,9 +99,9 @@ struct gg_context {
   long launches = 0;
   bool profiling = false;
   // per-kernel stats of the last build: [0] P0 contraction, [1] Sigma contraction
-  long kstat_launches[2] = {0, 0};
-  double kstat_seconds[2] = {0, 0};
-  double kstat_flops[2] = {0, 0};
+  long kstat_launches[3] = {0, 0, 0};
+  double kstat_seconds[3] = {0, 0, 0};
+  double kstat_flops[3] = {0, 0, 0};
 
   gg::SplitGemm* split = nullptr;
 

@@ -242,19 +242,19 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
   // the dominant contractions go through the split-precision engine when requested;
   // with profiling on, CUDA events bracket every such launch on `st`
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> kev;
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < 3; ++i) {
     c->kstat_launches[i] = 0;
     c->kstat_seconds[i] = 0.0;
     c->kstat_flops[i] = 0.0;
   }
-  auto gemm_main = [&](ZgemmDesc d, int which) {
+  auto gemm_main = [&](ZgemmDesc d, int which, bool allow_split = true) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c->profiling) {
       GG_CUDA(cudaEventCreate(&e0));
       GG_CUDA(cudaEventCreate(&e1));
       GG_CUDA(cudaEventRecord(e0, st));
     }
-    if (split) {
+    if (split && allow_split) {
       d.work = gw_work;
       d.work_elems = (long)c->gemm_work.n;
       c->launches += split_zgemm(split, d, c->slices, st);
@@ -489,7 +489,8 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
               gemm(d);
             }
             // Sigma[t][sp][kr][j][i] += -1/nk sum_Q sum_c Z[t][Q][j][c] conj(V[Q][i][c])
-            // (one GEMM over all tau: rows m = (t, j), V is the shared operand)
+            // (one GEMM over all tau: rows m = (t, j), V is the shared operand; FP64 in both
+            // precisions - slicing Z would move as many bytes as this GEMM takes)
             {
               ZgemmDesc d;
               d.M = T * n; d.N = n; d.K = n; d.KB = N;
@@ -499,7 +500,7 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
               d.c_m.split = n; d.c_m.hi = (long)ns * s.ink * nn; d.c_m.lo = n; d.c_n.lo = 1;
               d.alpha = make_double2(-1.0 / nk, 0.0);
               d.beta = make_double2(1.0, 0.0);
-              gemm(d);
+              gemm_main(d, 2, false);
             }
           }
         }

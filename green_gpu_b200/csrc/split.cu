@@ -79,21 +79,31 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// try_wait with a suspend-time hint: a warp whose phase is not complete is suspended (it
+// issues nothing, so the warps it shares a scheduler with keep their issue slots) until the
+// phase completes or about `ns` nanoseconds pass
+__device__ __forceinline__ bool mbar_try_sleep(uint64_t* b, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
 // bounded wait; returns false (and records `code`) on time-out or when another role failed
 // (abort_on_err = false for the teardown waits that must see in-flight work complete)
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* err, int code,
                                           bool abort_on_err = true) {
   if (mbar_try(b, parity)) return true;  // fast path: no clock read when the phase is complete
   const long long t0 = clock64();
-  int n = 0;
-  while (!mbar_try(b, parity)) {
-    if (++n == 64) {
-      n = 0;
-      if (abort_on_err && *err) return false;
-      if (clock64() - t0 > WAIT_CYCLES) {
-        atomicOr((int*)err, code);
-        return false;
-      }
+  while (!mbar_try_sleep(b, parity, 100000)) {  // <= 0.1 ms per suspension
+    if (abort_on_err && *err) return false;
+    if (clock64() - t0 > WAIT_CYCLES) {
+      atomicOr((int*)err, code);
+      return false;
     }
   }
   return true;
@@ -160,10 +170,12 @@ __device__ __forceinline__ void reg_fence8(int* r) {
   asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]));
 }
 
-// x * 2^e: one multiply by a constructed power of two while 2^e is a normal number
-__device__ __forceinline__ double scale_pow2(double x, int e) {
-  if (e >= -1022 && e <= 1023) return x * __longlong_as_double((long long)(e + 1023) << 52);
-  return ldexp(x, e);
+// 2^e as a double, e clamped to the normal range (operand exponents come from ilogb of
+// finite data, so a row factor times a column factor covers every representable result;
+// the clamp only matters for results that underflow or overflow anyway)
+__device__ __forceinline__ double pow2i(int e) {
+  e = max(-1022, min(1023, e));
+  return __longlong_as_double((long long)(e + 1023) << 52);
 }
 
 // drain `NC` int32 columns (a multiple of 8, at most 32) starting at taddr into acc * scale
@@ -228,6 +240,37 @@ __device__ __forceinline__ Unit unit_of(const I8Args& p, long u, int BN) {
   w.kb0 = (int)((unsigned)p.nkb * (unsigned)w.split / spl);
   w.kb1 = (int)((unsigned)p.nkb * (unsigned)(w.split + 1) / spl);
   return w;
+}
+
+// MMAs of one K block: every slice pair (s, t) with s + t = d into the accumulator of
+// diagonal d.  FIRST: the first K block of a segment (the first MMA of each diagonal
+// overwrites it, and with `reuse` it first waits until the epilogue has drained that
+// diagonal); LAST: the last K block (a commit per diagonal tells the epilogue that the
+// diagonal is complete).  Descriptor offsets are compile-time constants.
+template <int S, int BN, bool FIRST, bool LAST>
+__device__ __forceinline__ bool issue_kblock(uint32_t tacc0, uint64_t da, uint64_t db, uint32_t idesc, uint32_t leader,
+                                             bool reuse, uint64_t* acce, uint64_t* accf, uint32_t par_e,
+                                             volatile int* err) {
+#pragma unroll
+  for (int d = 2; d <= S + 1; ++d) {
+    if (FIRST && reuse) {
+      if (!__all_sync(0xffffffffu, mbar_wait(&acce[d - 2], par_e, err, 2))) return false;
+      tc_fence_after();
+    }
+    const uint32_t tacc = tacc0 + (uint32_t)((d - 2) * BN);
+    const int s_lo = d - S > 1 ? d - S : 1, s_hi = d - 1 < S ? d - 1 : S;
+#pragma unroll
+    for (int s = s_lo; s <= s_hi; ++s) {
+      const int t = d - s;
+#pragma unroll
+      for (int kk = 0; kk < KB / 32; ++kk)
+        mma_i8(tacc, da + (uint64_t)(((s - 1) * BM * KB) >> 4) + (uint64_t)(kk * 2),
+               db + (uint64_t)(((t - 1) * BN * KB) >> 4) + (uint64_t)(kk * 2), idesc,
+               (FIRST && s == s_lo && kk == 0) ? 0u : 1u, leader);
+    }
+    if (LAST) mma_commit(&accf[d - 2], leader);
+  }
+  return true;
 }
 
 // Persistent: one CTA per SM walks the work units u = blockIdx.x + i * gridDim.x.  The TMA
@@ -338,30 +381,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           tc_fence_after();
           const uint64_t da = dA0 + (uint64_t)((st * stA) >> 4);
           const uint64_t db = dB0 + (uint64_t)((st * stB) >> 4);
-#pragma unroll
-          for (int d = 2; d <= S + 1; ++d) {
-            if (reuse) {
-              // diagonal d of this set still holds the previous segment until it is drained
-              if (!__all_sync(0xffffffffu, mbar_wait(&acce[buf * ND + d - 2], par_e, err, 2))) {
-                ok = false;
-                break;
-              }
-              tc_fence_after();
-            }
-            const uint32_t tacc = tmem + (uint32_t)buf * buf_cols + (uint32_t)((d - 2) * BN);
-            const int s_lo = d - S > 1 ? d - S : 1, s_hi = d - 1 < S ? d - 1 : S;
-#pragma unroll
-            for (int s = s_lo; s <= s_hi; ++s) {
-              const int t = d - s;
-#pragma unroll
-              for (int kk = 0; kk < KB / 32; ++kk) {
-                const uint32_t accum = (first && s == s_lo && kk == 0) ? 0u : 1u;
-                mma_i8(tacc, da + (uint64_t)(((s - 1) * BM * KB) >> 4) + (uint64_t)(kk * 2),
-                       db + (uint64_t)(((t - 1) * BN * KB) >> 4) + (uint64_t)(kk * 2), idesc, accum, leader);
-              }
-            }
-            if (last) mma_commit(&accf[buf * ND + d - 2], leader);
-          }
+          const uint32_t tacc0 = tmem + (uint32_t)buf * buf_cols;
+          uint64_t* ae = acce + buf * ND;
+          uint64_t* af = accf + buf * ND;
+          if (!first && !last)
+            issue_kblock<S, BN, false, false>(tacc0, da, db, idesc, leader, false, ae, af, 0u, err);
+          else if (first && !last)
+            ok = issue_kblock<S, BN, true, false>(tacc0, da, db, idesc, leader, reuse, ae, af, par_e, err);
+          else if (!first)
+            issue_kblock<S, BN, false, true>(tacc0, da, db, idesc, leader, false, ae, af, 0u, err);
+          else
+            ok = issue_kblock<S, BN, true, true>(tacc0, da, db, idesc, leader, reuse, ae, af, par_e, err);
           if (!ok) break;
           mma_commit(&empty[st], leader);
           if (++st == p.stages) {
@@ -429,7 +459,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       const int b1 = (int)((w.batch / p.nb0) % p.nb1);
       const int b2 = (int)(w.batch / ((long)p.nb0 * p.nb1));
       const bool use_beta = p.beta.x != 0.0 || p.beta.y != 0.0;
+      const bool alpha_one = p.alpha.x == 1.0 && p.alpha.y == 0.0;
       const bool mok = m < p.M;
+      const double sa = pow2i(ea);  // row factor; x = 2 sum d_s 2^-7s per operand gives the + 2
       double2* crow = p.C + b0 * p.c_b0 + b1 * p.c_b1 + b2 * p.c_b2 + (mok ? p.c_m(m) : 0);
       double2* wrow = p.work + (w.split * p.batch + w.batch) * (long)p.N * p.M + m;
       // column offset c_n(n) stepped through the tile: (nq, nr) = divmod(n, split)
@@ -440,13 +472,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const int eb = __shfl_sync(0xffffffffu, eb_lane, c);
         const int n = nbase + c;
         if (mok && n < p.N) {
-          const int e = ea + eb + 2;  // x = 2 sum d_s 2^-7s per operand
-          const double2 v = make_double2(scale_pow2(acc[2 * c], e), scale_pow2(acc[2 * c + 1], e));
+          const double sb = pow2i(eb + 2);
+          const double2 v = make_double2(acc[2 * c] * sa * sb, acc[2 * c + 1] * sa * sb);
           if (p.splits > 1) {
             wrow[(long)n * p.M] = v;
           } else {
             double2* cp = crow + (p.c_n.split > 0 ? nq * p.c_n.hi + nr * p.c_n.lo : (long)n * p.c_n.lo);
-            double2 o = cmul(p.alpha, v);
+            double2 o = alpha_one ? v : cmul(p.alpha, v);
             if (use_beta) o = cadd(o, cmul(p.beta, *cp));
             *cp = o;
           }
@@ -572,7 +604,7 @@ template <bool BSIDE, int S>
 __global__ void slice_kernel(OpView v, int rows_pad, int ktiles, const int* ex, int8_t* out, long nbatch) {
   __shared__ double2 tile[32][33];
   const int Ktot = v.KB * v.K;
-  const int rtiles = rows_pad / 32;
+  const int rtiles = (rows_pad + 31) / 32;  // the last row tile may be partial
   long t = blockIdx.x;
   const int kt = (int)(t % ktiles);
   t /= ktiles;
@@ -618,6 +650,7 @@ __global__ void slice_kernel(OpView v, int rows_pad, int ktiles, const int* ex, 
   // write: thread (ty -> row, tx -> kk)
   for (int i = ty; i < 32; i += 8) {
     const int r = rt * 32 + i;
+    if (r >= rows_pad) break;
     const double2 x = tile[i][tx];
     const int e = (r < v.R) ? ex[b * (BSIDE ? v.R : rows_pad) + r] : 0;
     int8_t dr[S], di[S];
@@ -721,10 +754,10 @@ void launch_i8(const CUtensorMap& ta, const CUtensorMap& tb, const I8Args& a, lo
 template <int S>
 void launch_slices_s(const OpView& va, const OpView& vb, int rows_a_pad, int ncol_pad, int nkb, const int* ea,
                      const int* eb, int8_t* a8, int8_t* b8, long batch_a, long batch_b, cudaStream_t st) {
-  slice_kernel<false, S><<<(unsigned)((long)nkb * (rows_a_pad / 32) * batch_a), 256, 0, st>>>(va, rows_a_pad, nkb, ea,
+  slice_kernel<false, S><<<(unsigned)((long)nkb * ((rows_a_pad + 31) / 32) * batch_a), 256, 0, st>>>(va, rows_a_pad, nkb, ea,
                                                                                              a8, batch_a);
   GG_CHECK_LAUNCH();
-  slice_kernel<true, S><<<(unsigned)((long)nkb * (ncol_pad / 32) * batch_b), 256, 0, st>>>(vb, ncol_pad, nkb, eb, b8,
+  slice_kernel<true, S><<<(unsigned)((long)nkb * ((ncol_pad + 31) / 32) * batch_b), 256, 0, st>>>(vb, ncol_pad, nkb, eb, b8,
                                                                                           batch_b);
   GG_CHECK_LAUNCH();
 }
@@ -761,7 +794,6 @@ int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
   // BN <= 128 keeps the FP64 drain registers (BN / 2 per thread) in budget
   const int nbuf = S <= 2 ? 2 : 1;
   const int BN = S <= 4 ? 128 : S == 5 ? 96 : S == 6 ? 80 : 64;
-  const int bn_pad = BN * 64 / std::__gcd(BN, 64);  // keeps rows_b_pad / 2 a multiple of 32
   const long batch = (long)d.nb0 * d.nb1 * d.nb2;
   const long Ktot = (long)d.KB * d.K;
   if (2 * Ktot + KB >= (1L << 31) || (long)d.M >= (1L << 31) || (long)d.N >= (1L << 30))
@@ -769,7 +801,7 @@ int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
   const long kp = ((2 * Ktot + KB - 1) / KB) * KB;
   const int rows_a_pad = ((d.M + BM - 1) / BM) * BM;
   const int np = 2 * d.N;
-  const int rows_b_pad = ((np + bn_pad - 1) / bn_pad) * bn_pad;  // B' rows (2 per complex column)
+  const int rows_b_pad = ((np + BN - 1) / BN) * BN;  // B' rows (2 per complex column), whole tiles
   const int ncol_pad = rows_b_pad / 2;                // complex columns incl. padding
   // exact int32 chunk: S * Kchunk * 64^2 < 2^31 (slices are rounded, |d| <= 64)
   const long kchunk = std::max<long>(KB, ((2147483647L / (4096L * S)) / KB) * KB);

@@ -156,7 +156,8 @@ int gg_last_timings(const gg_context* ctx, double* out, int n);
 /* Per-kernel device time of the last GW build, from CUDA events recorded around every
  * launch of the named contraction on its stream when profiling is enabled:
  * which = 0: the P0 contraction (sum over k of A_k B_k^T), 1: the Sigma contraction
- * (W~ times (V G)).  Writes launches, total seconds and algorithmic flops
+ * (V times W~), 2: the final Sigma product with V^+ (reduction over Q and an orbital).
+ * Writes launches, total seconds and algorithmic flops
  * (8MNK + 12MN per complex GEMM, src/green/gpu/common_defs.h:121-125). */
 int gg_set_profiling(gg_context* ctx, int enable);
 int gg_kernel_stats(const gg_context* ctx, int which, int64_t* launches, double* seconds, double* flops);
