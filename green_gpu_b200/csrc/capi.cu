@@ -239,13 +239,43 @@ int gg_set_capture(gg_context* c, double* P0_out, double* Pw_out, double* Wt_out
   });
 }
 
+// GW build on device buffers in the reference layout; in X2C mode the spinor G is split into
+// its four spin blocks, the build runs on them as pseudo-spins and Sigma is reassembled
+static void gw_device(gg_context* c, const double2* G, double2* Sigma, int solver, int precision, cudaStream_t st) {
+  if (!c->x2c) {
+    gw_build(c, G, Sigma, solver, precision, st);
+    return;
+  }
+  x2c_check(c);
+  const auto& s = c->sh;
+  const size_t count = (size_t)s.nts * 4 * s.ink * s.nao * s.nao;
+  double2* g4 = c->x2c_in.ensure(count);
+  double2* s4 = c->x2c_out.ensure(count);
+  launch_x2c_split(G, s.nts, s.ink, s.nao, 4, g4, st);
+  gw_build(c, g4, s4, solver, precision, st);
+  launch_x2c_merge(s4, s.nts, s.ink, s.nao, 4, Sigma, st);
+}
+
+// matrices per (outer, spin, k) block of a G / Sigma / dm buffer: nao^2 x ns, or (2 nao)^2 in X2C
+static size_t spin_elems(const gg_context* c) {
+  const size_t nn = (size_t)c->sh.nao * c->sh.nao;
+  return c->x2c ? 4 * nn : (size_t)c->sh.ns * nn;
+}
+
+int gg_set_x2c(gg_context* c, int enable) {
+  return guarded(c, [&] {
+    if (enable && c->sh.ns != 1) throw Error(GG_ERR_ARG, "x2c: the spinor shape has ns = 1 (nso = 2 nao)");
+    c->x2c = enable != 0;
+  });
+}
+
 int gg_gw_sigma_device(gg_context* c, const void* G, void* Sigma, int solver, int precision, void* stream) {
   return guarded(c, [&] {
     if (!G || !Sigma) throw Error(GG_ERR_ARG, "gw: NULL buffer");
     if (((reinterpret_cast<uintptr_t>(G) | reinterpret_cast<uintptr_t>(Sigma)) & 15) != 0)
       throw Error(GG_ERR_ARG, "gw: device buffers must be 16-byte aligned");
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
-    gw_build(c, (const double2*)G, (double2*)Sigma, solver, precision, st);
+    gw_device(c, (const double2*)G, (double2*)Sigma, solver, precision, st);
   });
 }
 
@@ -253,7 +283,7 @@ int gg_gw_sigma(gg_context* c, const double* G, double* Sigma, int solver, int p
   return guarded(c, [&] {
     if (!G || !Sigma) throw Error(GG_ERR_ARG, "gw: NULL buffer");
     const auto& s = c->sh;
-    const size_t count = (size_t)s.nts * s.ns * s.ink * s.nao * s.nao;
+    const size_t count = (size_t)s.nts * s.ink * spin_elems(c);
     double2* gin = c->G_in.ensure(count);
     double2* sout = c->Sigma_out.ensure(count);
     cudaEvent_t e0, e1;
@@ -261,7 +291,7 @@ int gg_gw_sigma(gg_context* c, const double* G, double* Sigma, int solver, int p
     GG_CUDA(cudaEventCreate(&e1));
     GG_CUDA(cudaEventRecord(e0, c->stream));
     GG_CUDA(cudaMemcpyAsync(gin, G, count * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
-    gw_build(c, gin, sout, solver, precision, c->stream);
+    gw_device(c, gin, sout, solver, precision, c->stream);
     GG_CUDA(cudaMemcpyAsync(Sigma, sout, count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     GG_CUDA(cudaEventRecord(e1, c->stream));
     GG_CUDA(cudaStreamSynchronize(c->stream));
@@ -273,17 +303,43 @@ int gg_gw_sigma(gg_context* c, const double* G, double* Sigma, int solver, int p
   });
 }
 
+// density upload (split into the aa, bb, ab blocks in X2C mode: get_dm_fbz,
+// hf_gpu_kernel.cpp:326-336) and the engine's Fock buffer of hf_spins blocks
+static double2* hf_upload(gg_context* c, const double* dm, double2** F_blocks) {
+  const auto& s = c->sh;
+  const size_t count = (size_t)s.ink * spin_elems(c);
+  double2* din = c->G_in.ensure(std::max(count, c->G_in.n));
+  GG_CUDA(cudaMemcpyAsync(din, dm, count * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+  const size_t nblk = (size_t)hf_spins(c) * s.ink * s.nao * s.nao;
+  *F_blocks = c->hf_F.ensure(nblk);
+  if (!c->x2c) return din;
+  double2* d3 = c->x2c_in.ensure(std::max(nblk, c->x2c_in.n));
+  launch_x2c_split(din, 1, s.ink, s.nao, 3, d3, c->stream);
+  return d3;
+}
+
+// Fock blocks -> host in the caller's layout (X2C: spinor matrices, ba = ab^+,
+// copy_2c_Fock_from_device_to_host in cuda_common.cu:176-201)
+static void hf_download(gg_context* c, const double2* F_blocks, double* out) {
+  const auto& s = c->sh;
+  const size_t count = (size_t)s.ink * spin_elems(c);
+  const double2* src = F_blocks;
+  if (c->x2c) {
+    double2* f2 = c->x2c_out.ensure(std::max(count, c->x2c_out.n));
+    launch_x2c_merge(F_blocks, 1, s.ink, s.nao, 3, f2, c->stream);
+    src = f2;
+  }
+  GG_CUDA(cudaMemcpyAsync(out, src, count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  GG_CUDA(cudaStreamSynchronize(c->stream));
+}
+
 int gg_hf_exchange(gg_context* c, const double* dm, double* K_out) {
   return guarded(c, [&] {
     if (!dm || !K_out) throw Error(GG_ERR_ARG, "hf: NULL buffer");
-    const auto& s = c->sh;
-    const size_t count = (size_t)s.ns * s.ink * s.nao * s.nao;
-    double2* din = c->G_in.ensure(std::max(count, c->G_in.n));
-    double2* kout = c->hf_F.ensure(count);
-    GG_CUDA(cudaMemcpyAsync(din, dm, count * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    double2* kout = nullptr;
+    double2* din = hf_upload(c, dm, &kout);
     hf_exchange(c, din, kout, c->stream);
-    GG_CUDA(cudaMemcpyAsync(K_out, kout, count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
-    GG_CUDA(cudaStreamSynchronize(c->stream));
+    hf_download(c, kout, K_out);
   });
 }
 
@@ -291,36 +347,62 @@ int gg_hf_fock(gg_context* c, const double* dm, const double* S_k, double madelu
   return guarded(c, [&] {
     if (!dm || !S_k || !F_out) throw Error(GG_ERR_ARG, "hf: NULL buffer");
     const auto& s = c->sh;
-    const int n = s.nao;
-    const size_t nn = (size_t)n * n, count = (size_t)s.ns * s.ink * nn;
-    double2* din = c->G_in.ensure(std::max(count, c->G_in.n));
-    double2* fout = c->hf_F.ensure(count);
-    GG_CUDA(cudaMemcpyAsync(din, dm, count * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    double2* fout = nullptr;
+    double2* din = hf_upload(c, dm, &fout);
     hf_exchange(c, din, fout, c->stream);
     hf_direct(c, fout, c->stream);
+    const size_t m = c->x2c ? 2 * (size_t)s.nao : (size_t)s.nao, mm = m * m;
+    const size_t count = (size_t)s.ink * spin_elems(c);
     std::vector<double2> F(count);
-    GG_CUDA(cudaMemcpyAsync(F.data(), fout, count * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
-    GG_CUDA(cudaStreamSynchronize(c->stream));
-    // Ewald: F -= c * madelung * S D S per (s, IBZ k), c = 0.5 (ns = 1) or 1 (hf_gpu_kernel.cpp:188-201)
-    const double pre = (s.ns == 2 ? 1.0 : 0.5) * madelung;
+    hf_download(c, fout, reinterpret_cast<double*>(F.data()));
+    // Ewald on the host: F -= c * madelung * S D S per (s, IBZ k), c = 0.5 (ns = 1) or 1
+    // (hf_gpu_kernel.cpp:188-201).  X2C: per spin block with the AO overlap S_aa on both
+    // sides and c = 1; the ba block gets the adjoint of the ab term (hf_gpu_kernel.cpp:311-323)
     const double2* S = (const double2*)S_k;
     const double2* D = (const double2*)dm;
-    std::vector<double2> tmp(nn);
-    for (size_t b = 0; b < (size_t)s.ns * s.ink; ++b) {
-      const double2* Sb = S + b * nn;
-      const double2* Db = D + b * nn;
+    const int n = s.nao;
+    auto sds = [&](const double2* Sb, size_t sld, const double2* Db, size_t dld, double2* out) {
+      std::vector<double2> tmp((size_t)n * n);
       for (int i = 0; i < n; ++i)
         for (int j = 0; j < n; ++j) {
           double2 acc = make_double2(0, 0);
-          for (int a = 0; a < n; ++a) acc = cadd(acc, cmul(Sb[i * n + a], Db[a * n + j]));
-          tmp[i * n + j] = acc;
+          for (int a = 0; a < n; ++a) acc = cadd(acc, cmul(Sb[i * sld + a], Db[a * dld + j]));
+          tmp[(size_t)i * n + j] = acc;
         }
       for (int i = 0; i < n; ++i)
         for (int j = 0; j < n; ++j) {
           double2 acc = make_double2(0, 0);
-          for (int a = 0; a < n; ++a) acc = cadd(acc, cmul(tmp[i * n + a], Sb[a * n + j]));
-          F[b * nn + i * n + j] = csub(F[b * nn + i * n + j], cscale(acc, pre));
+          for (int a = 0; a < n; ++a) acc = cadd(acc, cmul(tmp[(size_t)i * n + a], Sb[a * sld + j]));
+          out[(size_t)i * n + j] = acc;
         }
+    };
+    std::vector<double2> E((size_t)n * n);
+    if (!c->x2c) {
+      const double pre = (s.ns == 2 ? 1.0 : 0.5) * madelung;
+      for (size_t b = 0; b < (size_t)s.ns * s.ink; ++b) {
+        sds(S + b * mm, m, D + b * mm, m, E.data());
+        for (size_t e = 0; e < mm; ++e) F[b * mm + e] = csub(F[b * mm + e], cscale(E[e], pre));
+      }
+    } else {
+      for (size_t k = 0; k < (size_t)s.ink; ++k) {
+        const double2* Sk = S + k * mm;  // S_aa block at (0, 0), leading dimension 2 nao
+        double2* Fk = F.data() + k * mm;
+        const int blocks[3][2] = {{0, 0}, {1, 1}, {0, 1}};
+        for (auto& bl : blocks) {
+          const int a = bl[0], b = bl[1];
+          sds(Sk, m, D + k * mm + (size_t)a * n * m + (size_t)b * n, m, E.data());
+          for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+              const double2 v = cscale(E[(size_t)i * n + j], madelung);
+              double2& f = Fk[(size_t)(a * n + i) * m + b * n + j];
+              f = csub(f, v);
+              if (a != b) {
+                double2& g = Fk[(size_t)(n + j) * m + i];
+                g = csub(g, make_double2(v.x, -v.y));
+              }
+            }
+        }
+      }
     }
     std::memcpy(F_out, F.data(), count * sizeof(double2));
   });

@@ -81,6 +81,10 @@ struct gg_context {
 
   int slices = 4;
   int hf_precision = GG_PREC_FP64;
+  // two-component (X2C) mode: inputs and outputs are spinor matrices of order 2 nao; GW runs
+  // on the four spin blocks as pseudo-spins (aa, bb, ab, ba), HF on three (aa, bb, ab)
+  int x2c = 0;
+  gg::DevBuf<double2> x2c_in, x2c_out;
   int shard_rank = 0, shard_size = 1;
 
   // capture of intermediates (host pointers)

@@ -143,8 +143,22 @@ void unfold_matrices(gg_context* c, const double2* X_in, int nouter, int ns, dou
   ++c->launches;
 }
 
+int gw_spins(const gg_context* c) { return c->x2c ? 4 : c->sh.ns; }
+int hf_spins(const gg_context* c) { return c->x2c ? 3 : c->sh.ns; }
+
+void x2c_check(const gg_context* c) {
+  if (!c->x2c) return;
+  bool tr = false;
+  for (auto v : c->k_tr) tr = tr || v != 0;
+  for (auto v : c->q_tr) tr = tr || v != 0;
+  if (c->has_Uk || c->has_Uq || tr)
+    throw Error(GG_ERR_ARG, "x2c: only the identity k/q symmetry is supported (no U_k / U_q rotations or "
+                            "time-reversal partners)");
+}
+
 Plan plan_gw(gg_context* c, int slices) {
   const auto& s = c->sh;
+  const int nspin = gw_spins(c);
   const size_t z = sizeof(double2);
   const size_t nn = (size_t)s.nao * s.nao, NN = (size_t)s.NQ * s.NQ, Nnn = (size_t)s.NQ * nn;
   const int T2 = s.nts / 2;
@@ -155,7 +169,7 @@ Plan plan_gw(gg_context* c, int slices) {
   p.dyson_batch = 4 * 148;
   auto need = [&](const Plan& q) {
     size_t b = 0;
-    b += 2 * (size_t)s.nk * s.ns * s.nts * nn;        // Gf + Gtmp
+    b += 2 * (size_t)s.nk * nspin * s.nts * nn;       // Gf + Gtmp
     b += (size_t)q.kc * Nnn;                           // Vbuf
     b += (size_t)q.kc * T2 * nn;                       // G1buf
     size_t p0s = (size_t)q.kc * q.tb * Nnn;            // A / B build buffers (each)
@@ -208,8 +222,13 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
   if (precision != GG_PREC_FP64 && precision != GG_PREC_SPLIT) throw Error(GG_ERR_ARG, "gw: unknown precision");
   if (solver != GG_SOLVER_CHOLESKY && solver != GG_SOLVER_LU) throw Error(GG_ERR_ARG, "gw: unknown solver");
   const auto& s = c->sh;
-  const int n = s.nao, N = s.NQ, T = s.nts, T2 = T / 2, nw = s.nw_b, nk = s.nk, ns = s.ns;
+  x2c_check(c);
+  const int n = s.nao, N = s.NQ, T = s.nts, T2 = T / 2, nw = s.nw_b, nk = s.nk, ns = gw_spins(c);
   const long nn = (long)n * n, NN = (long)N * N, Nnn = (long)N * nn;
+  // G^k(beta - tau) of pseudo-spin sp in the P0 operand build: the X2C pseudo-spins pair the
+  // (s1, s2) block of G^{k+q}(tau) with the (s2, s1) block of G^k(-tau), i.e. ab with ba
+  // (copy_Gk_2c with minus_t = true, gw_gpu_kernel.cpp:523-536)
+  auto spin_a = [&](int sp) { return (c->x2c && sp >= 2) ? 5 - sp : sp; };
   const Plan pl = plan_gw(c, precision == GG_PREC_SPLIT ? c->slices : 0);
   c->launches = 0;
 
@@ -338,7 +357,7 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
             {
               ZgemmDesc d;
               d.M = tn * n; d.N = N * n; d.K = n;
-              d.A = Gf + ((long)k0 * ns + sp) * T * nn + (long)(T - 1 - t0) * nn;
+              d.A = Gf + ((long)k0 * ns + spin_a(sp)) * T * nn + (long)(T - 1 - t0) * nn;
               d.a_m.split = n; d.a_m.hi = -nn; d.a_m.lo = n; d.a_k = 1;
               d.B = Vb; d.b_k = n; d.b_n.split = n; d.b_n.hi = nn; d.b_n.lo = 1;
               d.C = SA; d.c_m.split = n; d.c_m.hi = Nnn; d.c_m.lo = n;
@@ -534,8 +553,9 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
 void hf_exchange(gg_context* c, const double2* dm_dev, double2* K_dev, cudaStream_t st) {
   if (!c->has_sym || !c->has_kpairs || !c->V)
     throw Error(GG_ERR_STATE, "hf: symmetry, k-pairs and integrals must be set first");
+  x2c_check(c);
   const auto& s = c->sh;
-  const int n = s.nao, N = s.NQ, nk = s.nk, ns = s.ns;
+  const int n = s.nao, N = s.NQ, nk = s.nk, ns = hf_spins(c);
   const long nn = (long)n * n, Nnn = (long)N * nn;
   c->launches = 0;
   // unfolded density D[k][s][i][j]
@@ -598,7 +618,8 @@ void hf_exchange(gg_context* c, const double2* dm_dev, double2* K_dev, cudaStrea
 // (hf_gpu_kernel.cpp:141-186).  Uses the unfolded density left in c->hf_D by hf_exchange.
 void hf_direct(gg_context* c, double2* F_dev, cudaStream_t st) {
   const auto& s = c->sh;
-  const int n = s.nao, N = s.NQ, nk = s.nk, ns = s.ns;
+  // X2C: the density of the aa and bb blocks, J added to both (hf_gpu_kernel.cpp:269-309)
+  const int n = s.nao, N = s.NQ, nk = s.nk, ns = hf_spins(c), nsj = c->x2c ? 2 : ns;
   const long nn = (long)n * n, Nnn = (long)N * nn;
   double2* cq = c->hf_c.ensure(N);
   GG_CUDA(cudaMemsetAsync(cq, 0, sizeof(double2) * N, st));
@@ -618,7 +639,7 @@ void hf_direct(gg_context* c, double2* F_dev, cudaStream_t st) {
   for (int k0 = 0; k0 < nk; k0 += kc) {
     const int kn = std::min(kc, nk - k0);
     diag.gather(c, k0, kn, Vb, st);
-    for (int sp = 0; sp < ns; ++sp) {
+    for (int sp = 0; sp < nsj; ++sp) {
       launch_gather_blocks(c->hf_D.p, didx.d.p + (size_t)sp * nk + k0, kn, nn, nn, Dk, st);
       launch_hartree_coeff(Vb, Dk, kn, N, n, 1.0 / nk, cq, st);
     }
@@ -627,7 +648,7 @@ void hf_direct(gg_context* c, double2* F_dev, cudaStream_t st) {
   for (int kr = 0; kr < s.ink; ++kr) {
     diag.gather(c, (size_t)c->k_r2f[kr], 1, Vb, st);
     launch_hartree_apply(Vb, cq, N, n, J, st);
-    for (int sp = 0; sp < ns; ++sp) launch_axpy(F_dev + ((long)sp * s.ink + kr) * nn, J, nn, st);
+    for (int sp = 0; sp < nsj; ++sp) launch_axpy(F_dev + ((long)sp * s.ink + kr) * nn, J, nn, st);
   }
 }
 

@@ -500,6 +500,60 @@ void launch_gather_blocks(const double2* src, const int* idx, int nblocks, long 
   GG_CHECK_LAUNCH();
 }
 
+namespace {
+__device__ __forceinline__ void x2c_block(int ss, int& a, int& b) {
+  a = ss & 1;
+  b = (ss == 1 || ss == 2) ? 1 : 0;
+}
+
+__global__ void x2c_split_kernel(const double2* in, long nouter, long ninner, int n, int nblk, double2* out) {
+  const long nn = (long)n * n, total = nouter * nblk * ninner * nn;
+  const int n2 = 2 * n;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long ij = e % nn;
+    long r = e / nn;
+    const long kin = r % ninner;
+    r /= ninner;
+    const int ss = (int)(r % nblk);
+    const long o = r / nblk;
+    int a, b;
+    x2c_block(ss, a, b);
+    const int i = (int)(ij / n), j = (int)(ij % n);
+    out[e] = in[((o * ninner + kin) * n2 + a * n + i) * n2 + b * n + j];
+  }
+}
+
+__global__ void x2c_merge_kernel(const double2* in, long nouter, long ninner, int n, int nblk, double2* out) {
+  const int n2 = 2 * n;
+  const long nn = (long)n * n, mm = (long)n2 * n2, total = nouter * ninner * mm;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const int J = (int)(e % n2), I = (int)((e / n2) % n2);
+    const long r = e / mm, kin = r % ninner, o = r / ninner;
+    const int a = I >= n, b = J >= n, i = I - a * n, j = J - b * n;
+    // block index of (a, b): aa 0, bb 1, ab 2, ba 3
+    const int ss = (a == b) ? a : (a == 0 ? 2 : 3);
+    double2 v;
+    if (ss == 3 && nblk == 3) {
+      const double2 u = in[((o * nblk + 2) * ninner + kin) * nn + (long)j * n + i];
+      v = make_double2(u.x, -u.y);
+    } else {
+      v = in[((o * nblk + ss) * ninner + kin) * nn + (long)i * n + j];
+    }
+    out[e] = v;
+  }
+}
+}  // namespace
+
+void launch_x2c_split(const double2* in, long nouter, long ninner, int n, int nblk, double2* out, cudaStream_t st) {
+  x2c_split_kernel<<<grid_for(nouter * nblk * ninner * (long)n * n), TPB, 0, st>>>(in, nouter, ninner, n, nblk, out);
+  GG_CHECK_LAUNCH();
+}
+
+void launch_x2c_merge(const double2* in, long nouter, long ninner, int n, int nblk, double2* out, cudaStream_t st) {
+  x2c_merge_kernel<<<grid_for(nouter * ninner * 4L * n * n), TPB, 0, st>>>(in, nouter, ninner, n, nblk, out);
+  GG_CHECK_LAUNCH();
+}
+
 void launch_axpy(double2* y, const double2* x, long n, cudaStream_t st) {
   axpy_kernel<<<grid_for(n), TPB, 0, st>>>(y, x, n);
   GG_CHECK_LAUNCH();

@@ -24,6 +24,17 @@ void launch_gather_blocks(const double2* src, const int* idx_d, int nblocks, lon
 // y += x (n complex numbers)
 void launch_axpy(double2* y, const double2* x, long n, cudaStream_t st);
 
+// Two-component (X2C) spin blocks.  A spinor matrix of order 2n holds the blocks aa (0,0),
+// bb (n,n), ab (0,n) and ba (n,0).  Block ss of the pseudo-spin order is (row, col) =
+// (ss % 2, ss == 0 ? 0 : ss == 1 ? 1 : ss == 2 ? 1 : 0), i.e. aa, bb, ab, ba (the order of the
+// reference's copy_Gk_2c with minus_t = false and copy_Sigma_2c, gw_gpu_kernel.cpp:523-551,
+// cugw_qkpt.cu:382-403).
+// split: in [nouter][ninner][2n][2n] -> out [nouter][nblk][ninner][n][n] (nblk = 3 or 4)
+void launch_x2c_split(const double2* in, long nouter, long ninner, int n, int nblk, double2* out, cudaStream_t st);
+// merge: in [nouter][nblk][ninner][n][n] -> out [nouter][ninner][2n][2n]; with nblk = 3 the ba
+// block is the adjoint of ab (cuda_common.cu:176-201)
+void launch_x2c_merge(const double2* in, long nouter, long ninner, int n, int nblk, double2* out, cudaStream_t st);
+
 // scale: X *= s
 void launch_scale(double2* X, long n, double s, cudaStream_t st);
 void launch_fill_zero(double2* X, long n, cudaStream_t st);

@@ -17,7 +17,8 @@ Differences forced by the environment, kept explicit:
   stored k-pair array [num_kpair_stored][NQ][nao][nao]) or read from the reference's HDF5
   chunk files (``p["dfintegral_file"]`` / ``p["dfintegral_hf_file"]``, see df_integral.py);
 * ``ft`` is any object with ``Ttn_FB`` [nts][nw_b] and ``Tnt_BF`` [nw_b][nts-2].
-X2C (two-component) kernels are not built: ``X2C=True`` raises NotImplementedError.
+X2C (two-component) kernels (``X2C=True``, nso = 2 nao, ns = 1) run the C ABI's X2C mode
+(gg_set_x2c): the spin blocks as pseudo-spins, identity k/q symmetry only.
 """
 from __future__ import annotations
 
@@ -80,6 +81,16 @@ class scalar_hf_gpu_kernel:
         return self._ctx.hf_fock(dm, self._S_k, self._madelung)
 
 
+class x2c_hf_gpu_kernel(scalar_hf_gpu_kernel):
+    """x2c_hf_gpu_kernel (src/green/gpu/hf_gpu_kernel.h:68-100): spinor dm / Fock [1][ink][nso][nso]."""
+
+    def __init__(self, p, nao, nso, ns, NQ, madelung, bz_utils, S_k, verbose=1):
+        if nso != 2 * nao or ns != 1:
+            raise ValueError("x2c: nso = 2 nao and ns = 1")
+        super().__init__(p, nao, nso, ns, NQ, madelung, bz_utils, S_k, verbose)
+        self._ctx.set_x2c(True)
+
+
 class scalar_gw_gpu_kernel:
     """gw_gpu_kernel / scalar_gw_gpu_kernel (src/green/gpu/gw_gpu_kernel.h:40-206)."""
 
@@ -103,16 +114,23 @@ class scalar_gw_gpu_kernel:
         sigma[...] = out
 
 
+class x2c_gw_gpu_kernel(scalar_gw_gpu_kernel):
+    """x2c_gw_gpu_kernel (src/green/gpu/gw_gpu_kernel.h:131-206): spinor G / Sigma [nts][1][ink][nso][nso]."""
+
+    def __init__(self, p, nao, nso, ns, NQ, ft, bz_utils, cuda_lin_solver="LU", verbose=1):
+        if nso != 2 * nao or ns != 1:
+            raise ValueError("x2c: nso = 2 nao and ns = 1")
+        super().__init__(p, nao, nso, ns, NQ, ft, bz_utils, cuda_lin_solver, verbose)
+        self._ctx.set_x2c(True)
+
+
 def custom_hf_kernel(X2C, p, nao, nso, ns, NQ, madelung, bz_utils, S_k):
-    if X2C:
-        raise NotImplementedError("X2C HF kernel is not built")
-    kernel = scalar_hf_gpu_kernel(p, nao, nso, ns, NQ, madelung, bz_utils, S_k)
+    cls = x2c_hf_gpu_kernel if X2C else scalar_hf_gpu_kernel
+    kernel = cls(p, nao, nso, ns, NQ, madelung, bz_utils, S_k)
     return kernel, kernel.solve
 
 
 def custom_gw_kernel(X2C, p, nao, nso, ns, NQ, ft, bz_utils, S_k):
-    if X2C:
-        raise NotImplementedError("X2C GW kernel is not built")
-    kernel = scalar_gw_gpu_kernel(p, nao, nso, ns, NQ, ft, bz_utils, p.get("cuda_linear_solver", "LU"),
-                                  p.get("verbose", 0))
+    cls = x2c_gw_gpu_kernel if X2C else scalar_gw_gpu_kernel
+    kernel = cls(p, nao, nso, ns, NQ, ft, bz_utils, p.get("cuda_linear_solver", "LU"), p.get("verbose", 0))
     return kernel, kernel.solve

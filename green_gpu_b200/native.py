@@ -31,7 +31,7 @@ EXPORTS = [
     "gg_set_coulomb_device", "gg_set_ir", "gg_set_split_slices", "gg_gw_sigma", "gg_gw_sigma_device",
     "gg_set_capture", "gg_hf_exchange", "gg_hf_fock", "gg_symmetry_unfold", "gg_last_timings", "gg_version",
     "gg_set_profiling", "gg_kernel_stats", "gg_last_launch_count", "gg_set_q_shard", "gg_zgemm",
-    "gg_zgemm_noalloc", "gg_set_hf_precision", "gg_estimate_bytes",
+    "gg_zgemm_noalloc", "gg_set_hf_precision", "gg_estimate_bytes", "gg_set_x2c",
 ]
 
 
@@ -84,6 +84,7 @@ def load(path: str = LIB_PATH):
         "gg_zgemm": (C.c_int, [P, C.c_int64, C.c_int64, C.c_int64, D, D, D, C.c_int]),
         "gg_zgemm_noalloc": (C.c_int, [C.c_int64, C.c_int64, C.c_int64, P, P, P, P]),
         "gg_set_hf_precision": (C.c_int, [P, C.c_int]),
+        "gg_set_x2c": (C.c_int, [P, C.c_int]),
         "gg_estimate_bytes": (C.c_int, [C.POINTER(Shape), C.c_int64, C.POINTER(C.c_int64)]),
     }
     for name, (res, args) in sig.items():
@@ -174,13 +175,24 @@ class Context:
     def set_hf_precision(self, precision: int):
         self._check(self.lib.gg_set_hf_precision(self.h, int(precision)))
 
+    def set_x2c(self, enable: bool = True):
+        """Two-component mode: G / Sigma / dm / S_k / Fock are spinor matrices of order 2 nao."""
+        self._check(self.lib.gg_set_x2c(self.h, int(bool(enable))))
+        self.x2c = bool(enable)
+
+    def _mat(self):
+        """(spin blocks, matrix order) of the caller's G / dm layout."""
+        s = self.shape
+        return (1, 2 * s.nao) if getattr(self, "x2c", False) else (s.ns, s.nao)
+
     def set_split_slices(self, slices: int):
         self._check(self.lib.gg_set_split_slices(self.h, int(slices)))
 
     # --- compute --------------------------------------------------------------------
     def gw_sigma(self, G_tskij, solver=SOLVER_CHOLESKY, precision=PREC_FP64, capture=False):
         s = self.shape
-        shp = (s.nts, s.ns, s.ink, s.nao, s.nao)
+        ns_, m = self._mat()
+        shp = (s.nts, ns_, s.ink, m, m)
         G = _c128(G_tskij, shp)
         out = np.empty(shp, np.complex128)
         cap = None
@@ -204,7 +216,8 @@ class Context:
 
     def hf_exchange(self, dm):
         s = self.shape
-        shp = (s.ns, s.ink, s.nao, s.nao)
+        ns_, m = self._mat()
+        shp = (ns_, s.ink, m, m)
         D = _c128(dm, shp)
         out = np.empty(shp, np.complex128)
         self._check(self.lib.gg_hf_exchange(self.h, _d(D.view(np.float64)), _d(out.view(np.float64))))
@@ -212,7 +225,8 @@ class Context:
 
     def hf_fock(self, dm, S_k, madelung):
         s = self.shape
-        shp = (s.ns, s.ink, s.nao, s.nao)
+        ns_, m = self._mat()
+        shp = (ns_, s.ink, m, m)
         D = _c128(dm, shp)
         S = _c128(S_k, shp)
         out = np.empty(shp, np.complex128)

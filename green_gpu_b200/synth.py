@@ -319,3 +319,32 @@ def coulomb_pair(sys_: System, k1: int, k2: int) -> np.ndarray:
     elif trans:
         V = np.swapaxes(V, -1, -2)
     return np.ascontiguousarray(V)
+
+
+def make_x2c_system(mesh=(2, 1, 1), nao=6, NQ=20, beta=10.0, lam=100.0, nts=24, nw_b=21, seed=0,
+                    spin_orbit=0.3) -> System:
+    """Two-component system: the scalar system's integrals, IR transforms and identity symmetry,
+    with spinor G(tau) [nts][1][ink][2 nao][2 nao] from random Hermitian spinor Fock matrices
+    whose spin blocks are coupled (the ab block scaled by ``spin_orbit``) and a spin-independent
+    overlap S_k = diag(S, S).  ``nao`` counts orbitals per spin."""
+    base = make_system(mesh=mesh, nao=nao, NQ=NQ, ns=1, beta=beta, lam=lam, nts=nts, nw_b=nw_b, seed=seed,
+                       symmetry="none")
+    rng = np.random.default_rng(seed + 1000)
+    n2 = 2 * nao
+    G = np.zeros((nts, 1, base.ink, n2, n2), np.complex128)
+    S = np.zeros((1, base.ink, n2, n2), np.complex128)
+    for ik in range(base.ink):
+        X = rng.standard_normal((n2, n2)) + 1j * rng.standard_normal((n2, n2))
+        X[:nao, nao:] *= spin_orbit
+        X[nao:, :nao] *= spin_orbit
+        Fk = 0.5 * (X + X.conj().T)
+        eps, Q = np.linalg.eigh(Fk)
+        F = (Q * rng.uniform(-2.0, 2.0, n2)) @ Q.conj().T
+        F = 0.5 * (F + F.conj().T)
+        G[:, 0, ik] = _green_tau(F, base.tau, beta)
+        S[0, ik, :nao, :nao] = base.S_k[0, ik]
+        S[0, ik, nao:, nao:] = base.S_k[0, ik]
+    base.G_tskij = G
+    base.S_k = S
+    base.meta = dict(base.meta, x2c=True)
+    return base

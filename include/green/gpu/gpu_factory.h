@@ -42,7 +42,10 @@ namespace green::gpu {
 
   namespace detail {
     // symmetry tables exactly as make_cu_symmetry_data builds them (gw_gpu_kernel.cpp:34-91)
-    inline void set_symmetry(green::b200::context& ctx, const bz_utils_t& bz, size_t nao, size_t NQ, bool with_uq) {
+    // x2c: the spinor transformations are not applied (gg_set_x2c accepts only the identity
+    // symmetry), so no U_k / U_q are uploaded
+    inline void set_symmetry(green::b200::context& ctx, const bz_utils_t& bz, size_t nao, size_t NQ, bool with_uq,
+                             bool x2c = false) {
       const auto& ks = bz.k_symmetry();
       const auto& qs = bz.q_symmetry();
       const auto& kq = bz.k_q_map();
@@ -70,7 +73,7 @@ namespace green::gpu {
       }
       ctx.set_symmetry(to64(ks.full_to_reduced()), to64(ks.reduced_to_full()), to64(ks.tr_conj_list()),
                        to64(qs.full_to_reduced()), to64(qs.reduced_to_full()), to64(qs.tr_conj_list()), k1, k2,
-                       Uk.data(), with_uq ? Uq.data() : nullptr);
+                       x2c ? nullptr : Uk.data(), (with_uq && !x2c) ? Uq.data() : nullptr);
       const size_t npairs = nk * (nk + 1) / 2;
       std::vector<int64_t> conj(npairs), trans(npairs), pos(npairs);
       for (size_t i = 0; i < npairs; ++i) {
@@ -123,10 +126,12 @@ namespace green::gpu {
   // hf_gpu_kernel::solve (hf_gpu_kernel.cpp:66-104): returns exchange + direct - Ewald
   class scalar_hf_gpu_kernel {
   public:
+    // x2c = true is x2c_hf_gpu_kernel (hf_gpu_kernel.h:68-100): nso = 2 nao, ns = 1
     scalar_hf_gpu_kernel(const params::params& p, size_t nao, size_t nso, size_t ns, size_t NQ, double madelung,
-                         const bz_utils_t& bz, const ztensor<4>& S_k) :
+                         const bz_utils_t& bz, const ztensor<4>& S_k, bool x2c = false) :
         _ctx(detail::shape(bz, nao, NQ, ns, 4, 0)), _madelung(madelung), _S_k(S_k), _ns(ns), _ink(bz.ink()), _nso(nso) {
-      detail::set_symmetry(_ctx, bz, nao, NQ, false);
+      detail::set_symmetry(_ctx, bz, nao, NQ, false, x2c);
+      if (x2c) _ctx.set_x2c(true);
       auto V = detail::read_integrals(p["dfintegral_hf_file"], bz.k_symmetry().num_kpair_stored(), nao, NQ);
       _ctx.set_coulomb(V.data());
     }
@@ -146,13 +151,16 @@ namespace green::gpu {
   // gw_gpu_kernel::solve (gw_gpu_kernel.cpp:163-205): overwrites sigma with Sigma(tau)
   class scalar_gw_gpu_kernel {
   public:
+    // x2c = true is x2c_gw_gpu_kernel (gw_gpu_kernel.h:131-206): nso = 2 nao, ns = 1
     scalar_gw_gpu_kernel(const params::params& p, size_t nao, size_t nso, size_t ns, size_t NQ,
-                         const grids::transformer_t& ft, const bz_utils_t& bz, LinearSolverType solver, int verbose = 1) :
+                         const grids::transformer_t& ft, const bz_utils_t& bz, LinearSolverType solver, int verbose = 1,
+                         bool x2c = false) :
         _ctx(detail::shape(bz, nao, NQ, ns, ft.sd().repn_fermi().nts(), ft.sd().repn_bose().nw())),
         _solver(solver == LinearSolverType::Cholesky ? GG_SOLVER_CHOLESKY : GG_SOLVER_LU),
         _precision((p["P_sp"].as<bool>() && p["Sigma_sp"].as<bool>()) ? GG_PREC_SPLIT : GG_PREC_FP64) {
       if (ft.sd().repn_fermi().nts() % 2 != 0) throw std::runtime_error("Number of tau points should be even number");
-      detail::set_symmetry(_ctx, bz, nao, NQ, true);
+      detail::set_symmetry(_ctx, bz, nao, NQ, true, x2c);
+      if (x2c) _ctx.set_x2c(true);
       auto V = detail::read_integrals(p["dfintegral_file"], bz.k_symmetry().num_kpair_stored(), nao, NQ);
       _ctx.set_coulomb(V.data());
       _ctx.set_ir(ft.Ttn_FB().data(), ft.Tnt_BF().data());
@@ -171,8 +179,7 @@ namespace green::gpu {
   inline std::tuple<std::shared_ptr<void>, std::function<x_type(const x_type&)>> custom_hf_kernel(
       bool X2C, const params::params& p, size_t nao, size_t nso, size_t ns, size_t NQ, double madelung,
       const bz_utils_t& bz_utils, const ztensor<4>& S_k) {
-    if (X2C) throw std::logic_error("green-b200: X2C HF kernel is not built");
-    std::shared_ptr<void> kernel(new scalar_hf_gpu_kernel(p, nao, nso, ns, NQ, madelung, bz_utils, S_k));
+    std::shared_ptr<void> kernel(new scalar_hf_gpu_kernel(p, nao, nso, ns, NQ, madelung, bz_utils, S_k, X2C));
     std::function<x_type(const x_type&)> callback = [kernel](const x_type& dm) -> x_type {
       return static_cast<scalar_hf_gpu_kernel*>(kernel.get())->solve(dm);
     };
@@ -182,9 +189,8 @@ namespace green::gpu {
   inline std::tuple<std::shared_ptr<void>, std::function<void(G_type&, G_type&)>> custom_gw_kernel(
       bool X2C, const params::params& p, size_t nao, size_t nso, size_t ns, size_t NQ, const grids::transformer_t& ft,
       const bz_utils_t& bz_utils, const ztensor<4>& S_k) {
-    if (X2C) throw std::logic_error("green-b200: X2C GW kernel is not built");
     std::shared_ptr<void> kernel(
-        new scalar_gw_gpu_kernel(p, nao, nso, ns, NQ, ft, bz_utils, p["cuda_linear_solver"], p["verbose"]));
+        new scalar_gw_gpu_kernel(p, nao, nso, ns, NQ, ft, bz_utils, p["cuda_linear_solver"], p["verbose"], X2C));
     std::function<void(G_type&, G_type&)> callback = [kernel](G_type& g, G_type& s) {
       static_cast<scalar_gw_gpu_kernel*>(kernel.get())->solve(g, s);
     };

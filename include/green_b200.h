@@ -135,6 +135,17 @@ int gg_set_capture(gg_context* ctx, double* P0_out, double* Pw_out, double* Wt_o
  * reference's HF path is FP64 only (cuhf_utils.cu). */
 int gg_set_hf_precision(gg_context* ctx, int precision);
 
+/* Two-component (X2C) mode, replacing x2c_gw_gpu_kernel / x2c_hf_gpu_kernel
+ * (src/gw_gpu_kernel.cpp:457-551, src/hf_gpu_kernel.cpp:229-338; selected by the X2C flag of
+ * custom_gw_kernel / custom_hf_kernel, gpu_factory.h:47-89).  The context is created with
+ * ns = 1 and nao = the number of orbitals per spin; G, Sigma, dm, S_k and the Fock matrix are
+ * then spinor matrices of order nso = 2 nao: G/Sigma [nts][1][ink][nso][nso], dm/S_k/F
+ * [1][ink][nso][nso].  GW runs on the spin blocks aa, bb, ab, ba as four pseudo-spins (P0
+ * prefactor -1, the ab block of G(tau) paired with the ba block of G(-tau)); HF on aa, bb, ab
+ * (prefactor -1, ba = ab^+), the Hartree term from aa + bb added to aa and bb, Ewald per block
+ * with S_aa.  Only the identity k/q symmetry is accepted (GG_ERR_ARG otherwise). */
+int gg_set_x2c(gg_context* ctx, int enable);
+
 /* Exchange part K_s(k) [ns][ink][nao][nao] for the IBZ density dm [ns][ink][nao][nao]
  * (host buffers). */
 int gg_hf_exchange(gg_context* ctx, const double* dm, double* K_out);

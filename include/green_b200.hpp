@@ -55,6 +55,7 @@ public:
     check(gg_set_ir(h_, reinterpret_cast<const double*>(Ttn_FB), reinterpret_cast<const double*>(Tnt_BF)));
   }
   void set_split_slices(int s) { check(gg_set_split_slices(h_, s)); }
+  void set_x2c(bool on) { check(gg_set_x2c(h_, on ? 1 : 0)); }
   void set_q_shard(int rank, int size) { check(gg_set_q_shard(h_, rank, size)); }
   void gw_sigma(const cplx* G, cplx* Sigma, int solver = GG_SOLVER_CHOLESKY, int precision = GG_PREC_FP64) {
     check(gg_gw_sigma(h_, reinterpret_cast<const double*>(G), reinterpret_cast<double*>(Sigma), solver, precision));

@@ -63,3 +63,27 @@ def load(path=None, gw=False, nw_b=None):
     )
     ref = {"Sigma1": d["Sigma1"], "Fock_k_full": d["Fock_k_full"], "Sigma_tau_gw": d["Sigma_tau_gw"]}
     return sys_, ref
+
+
+def load_x2c(path=None):
+    """``hf_x2c_gamma.npz``: the reference's HF_X2C fixture (one k point, identity symmetry) as a
+    System with nao = orbitals per spin and ns = 1, plus dm [1][1][2n][2n] and Sigma1."""
+    d = np.load(path or os.path.join(HERE, "hf_x2c_gamma.npz"))
+    nk, NQ, nao = int(d["nk"]), int(d["NQ"]), int(d["nao"])
+    assert nk == 1 and int(d["ink"]) == 1
+    # the stored transforms are identities: the identity symmetry is used
+    assert np.allclose(d["U_k"][0], np.eye(2 * nao)) and np.allclose(d["U_q"][0], np.eye(NQ))
+    assert not np.any(d["k_tr_conj"]) and not np.any(d["q_tr_conj"])
+    one = np.zeros(1, np.int64)
+    sys_ = System(
+        nk=1, ink=1, nq=1, inq=1, nao=nao, NQ=NQ, ns=1, nts=4, nw_b=0, beta=100.0,
+        k_full_to_reduced=one, k_reduced_to_full=one, k_tr_conj=one, k_stars=[one],
+        q_full_to_reduced=one, q_reduced_to_full=one, q_tr_conj=one, q_stars=[one],
+        k1_from_k2q=one, k2_from_k1q=one, U_k=None, U_q=None,
+        conj_kpair_list=one, trans_kpair_list=one, irre_pos_kpair=one,
+        V_stored=np.ascontiguousarray(d["V_stored"]), G_tskij=np.zeros((4, 1, 1, 2 * nao, 2 * nao), np.complex128),
+        Ttn_FB=np.zeros((4, 0), np.complex128), Tnt_BF=np.zeros((0, 2), np.complex128),
+        S_k=np.ascontiguousarray(d["S_k"]), madelung=float(d["madelung"]),
+        meta={"fixture": "X2C, one k point (reference test/data/HF_X2C)"},
+    )
+    return sys_, {"dm": np.ascontiguousarray(d["dm"]), "Sigma1": d["Sigma1"]}

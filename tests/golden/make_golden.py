@@ -5,7 +5,8 @@ Run in a container where the reference tree is mounted read-only at
 
     python tests/golden/make_golden.py [/root/reference]
 
-Reads ``test/data/HF/{input.h5,data.h5,df_hf_int/*}`` and ``test/data/GW/data.h5``
+Reads ``test/data/HF/{input.h5,data.h5,df_hf_int/*}``, ``test/data/GW/data.h5`` and
+``test/data/HF_X2C/*`` (written to ``hf_x2c_gamma.npz``)
 (the inputs of ``solve_hf`` / ``Symmetry_Transform`` in
 test/cu_solver_test.cpp:34-96, 343-412) and writes ``hf_h2_27k.npz`` next to
 this script.  The file holds the k/q symmetry tables, the stored
@@ -65,6 +66,34 @@ def main(ref_root="/root/reference"):
     out["U_k"] = inp["symmetry/k/k_sym_transform_ao"]
     out["U_q"] = inp["symmetry/q/k_sym_transform_p0"]
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "hf_h2_27k.npz")
+    np.savez_compressed(dst, **out)
+    print("wrote", dst, os.path.getsize(dst), "bytes")
+    x2c(base)
+
+
+def x2c(base):
+    """HF_X2C fixture (test/cu_solver_test.cpp:335-337 -> solve_hf, :34-96): one k point,
+    10 orbitals per spin (nso 20), NQ 154.  Stores the density dm = G_tau[last] (the only
+    slice solve_hf reads), S_k, the stored integrals and result/Sigma1."""
+    inp = H5File(os.path.join(base, "HF_X2C", "input.h5"))
+    dat = H5File(os.path.join(base, "HF_X2C", "data.h5"))
+    raw = H5File(os.path.join(base, "HF_X2C", "df_hf_int", "VQ_0.h5"))["/0"]
+
+    def cplx(a):
+        a = np.asarray(a)
+        return a[..., 0] + 1j * a[..., 1]
+
+    G = dat["G_tau"]
+    out = {
+        "nao": int(inp["params/nao"]), "nso": int(inp["params/nso"]), "ns": int(inp["params/ns"]),
+        "nk": int(inp["params/nk"]), "NQ": int(inp["params/NQ"]), "ink": int(inp["symmetry/k/ink"]),
+        "madelung": float(inp["HF/madelung"]), "S_k": cplx(inp["HF/S-k"]),
+        "V_stored": raw[..., 0::2] + 1j * raw[..., 1::2], "dm": np.asarray(G[G.shape[0] - 1]),
+        "Sigma1": dat["result/Sigma1"],
+        "U_k": inp["symmetry/k/k_sym_transform_ao"], "U_q": inp["symmetry/q/k_sym_transform_p0"],
+        "k_tr_conj": inp["symmetry/k/tr_conj"], "q_tr_conj": inp["symmetry/q/tr_conj"],
+    }
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "hf_x2c_gamma.npz")
     np.savez_compressed(dst, **out)
     print("wrote", dst, os.path.getsize(dst), "bytes")
 

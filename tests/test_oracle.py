@@ -130,3 +130,47 @@ def test_df_integral_reader_matches_fixture():
     s, _ = fixture.load()
     V = df_integral.read_stored(ref_dir, s.nao, s.NQ)
     assert np.array_equal(V, s.V_stored)
+
+
+def test_x2c_hf_oracle_matches_reference_sigma1():
+    # test/cu_solver_test.cpp:335-337 (HF_X2C): Sigma1 = -1 * solve(dm), dm = G_tau[last],
+    # compared element-wise at an absolute 1e-8.
+    from oracle import x2c
+    s, ref = fixture.load_x2c()
+    out = -1.0 * x2c.hf_build(s, ref["dm"])
+    assert np.abs(out - ref["Sigma1"]).max() < 1e-8
+
+
+def _blockdiag(X, Y):
+    n = X.shape[-1]
+    out = np.zeros(X.shape[:-2] + (2 * n, 2 * n), np.complex128)
+    out[..., :n, :n] = X
+    out[..., n:, n:] = Y
+    return out
+
+
+def test_x2c_oracle_spin_diagonal_equals_scalar():
+    # with uncoupled spins (ab = ba = 0) the two-component build reduces to the scalar one:
+    # P0 sums the aa and bb blocks with prefactor -1 where the scalar build doubles one block
+    # with -2; HF takes each spin block at half the scalar (spin-summed) density.
+    from oracle import x2c
+    s = _tiny("none")
+    sig = gw.gw_build(s)
+    S2 = _blockdiag(s.G_tskij[:, 0], s.G_tskij[:, 0])[:, None]
+    out = x2c.gw_build(s, S2)
+    assert np.abs(out - _blockdiag(sig[:, 0], sig[:, 0])[:, None]).max() < 1e-12 * np.abs(sig).max()
+    dm = s.G_tskij[-1]
+    F = hf.hf_build(s, dm)
+    s2 = _tiny("none")
+    s2.S_k = _blockdiag(s.S_k, s.S_k)
+    F2 = x2c.hf_build(s2, _blockdiag(0.5 * dm, 0.5 * dm))
+    assert np.abs(F2 - _blockdiag(F, F)).max() < 1e-12 * np.abs(F).max()
+
+
+def test_x2c_split_merge_roundtrip():
+    from oracle import x2c
+    rng = np.random.default_rng(5)
+    M = rng.standard_normal((3, 8, 8)) + 1j * rng.standard_normal((3, 8, 8))
+    assert np.array_equal(x2c.merge(x2c.split(M, 4)), M)
+    H = M + np.conj(np.swapaxes(M, 1, 2))
+    assert np.array_equal(x2c.merge(x2c.split(H, 3)), H)
