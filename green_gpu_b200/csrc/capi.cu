@@ -3,6 +3,7 @@
 // the message for gg_last_error().
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include "context.cuh"
@@ -97,6 +98,7 @@ int gg_set_symmetry(gg_context* c, const int64_t* k_f2r, const int64_t* k_r2f, c
                     const int64_t* q_f2r, const int64_t* q_r2f, const int64_t* q_tr, const int64_t* k1q,
                     const int64_t* k2q, const double* U_k, const double* U_q) {
   return guarded(c, [&] {
+    c->invalidate();  // tables and captured graph depend on this setting
     if (!k_f2r || !k_r2f || !k_tr || !q_f2r || !q_r2f || !q_tr || !k1q || !k2q)
       throw Error(GG_ERR_ARG, "symmetry: index arrays must not be NULL");
     const auto& s = c->sh;
@@ -146,6 +148,7 @@ int gg_set_symmetry(gg_context* c, const int64_t* k_f2r, const int64_t* k_r2f, c
 int gg_set_kpairs(gg_context* c, int64_t nstored, const int64_t* conj_list, const int64_t* trans_list,
                   const int64_t* irre_pos) {
   return guarded(c, [&] {
+    c->invalidate();  // tables and captured graph depend on this setting
     if (!conj_list || !trans_list || !irre_pos || nstored <= 0) throw Error(GG_ERR_ARG, "kpairs: bad arguments");
     const long npairs = (long)c->sh.nk * (c->sh.nk + 1) / 2;
     for (long i = 0; i < npairs; ++i) {
@@ -163,6 +166,7 @@ int gg_set_kpairs(gg_context* c, int64_t nstored, const int64_t* conj_list, cons
 
 int gg_set_coulomb(gg_context* c, const double* V) {
   return guarded(c, [&] {
+    c->invalidate();  // tables and captured graph depend on this setting
     if (!V) throw Error(GG_ERR_ARG, "coulomb: NULL");
     if (!c->has_kpairs) throw Error(GG_ERR_STATE, "coulomb: call gg_set_kpairs first");
     const size_t count = (size_t)c->nstored * c->sh.NQ * c->sh.nao * c->sh.nao;
@@ -174,6 +178,7 @@ int gg_set_coulomb(gg_context* c, const double* V) {
 
 int gg_set_coulomb_device(gg_context* c, const void* V) {
   return guarded(c, [&] {
+    c->invalidate();  // tables and captured graph depend on this setting
     if (!V) throw Error(GG_ERR_ARG, "coulomb: NULL");
     if ((reinterpret_cast<uintptr_t>(V) & 15) != 0) throw Error(GG_ERR_ARG, "coulomb: device pointer not 16-byte aligned");
     if (!c->has_kpairs) throw Error(GG_ERR_STATE, "coulomb: call gg_set_kpairs first");
@@ -188,6 +193,7 @@ int gg_set_coulomb_device(gg_context* c, const void* V) {
 
 int gg_set_ir(gg_context* c, const double* Ttn_FB, const double* Tnt_BF) {
   return guarded(c, [&] {
+    c->invalidate();  // tables and captured graph depend on this setting
     if (!Ttn_FB || !Tnt_BF) throw Error(GG_ERR_ARG, "ir: NULL");
     if (c->sh.nw_b <= 0) throw Error(GG_ERR_ARG, "ir: the context was created with nw_b = 0");
     const int T = c->sh.nts, T2 = T / 2, nw = c->sh.nw_b;
@@ -218,6 +224,7 @@ int gg_set_hf_precision(gg_context* c, int precision) {
 
 int gg_set_q_shard(gg_context* c, int rank, int size) {
   return guarded(c, [&] {
+    c->invalidate();  // tables and captured graph depend on this setting
     if (size < 1 || rank < 0 || rank >= size) throw Error(GG_ERR_ARG, "q shard: need 0 <= rank < size");
     c->shard_rank = rank;
     c->shard_size = size;
@@ -226,6 +233,7 @@ int gg_set_q_shard(gg_context* c, int rank, int size) {
 
 int gg_set_split_slices(gg_context* c, int slices) {
   return guarded(c, [&] {
+    c->invalidate();  // tables and captured graph depend on this setting
     if (slices < 2 || slices > 8) throw Error(GG_ERR_ARG, "split slices must be in [2, 8]");
     c->slices = slices;
   });
@@ -241,7 +249,7 @@ int gg_set_capture(gg_context* c, double* P0_out, double* Pw_out, double* Wt_out
 
 // GW build on device buffers in the reference layout; in X2C mode the spinor G is split into
 // its four spin blocks, the build runs on them as pseudo-spins and Sigma is reassembled
-static void gw_device(gg_context* c, const double2* G, double2* Sigma, int solver, int precision, cudaStream_t st) {
+static void gw_sequence(gg_context* c, const double2* G, double2* Sigma, int solver, int precision, cudaStream_t st) {
   if (!c->x2c) {
     gw_build(c, G, Sigma, solver, precision, st);
     return;
@@ -256,6 +264,65 @@ static void gw_device(gg_context* c, const double2* G, double2* Sigma, int solve
   launch_x2c_merge(s4, s.nts, s.ink, s.nao, 4, Sigma, st);
 }
 
+}  // extern "C"
+
+// capture f() (work issued on `st`, and on streams joined to it) into an executable graph
+template <typename F>
+static cudaGraphExec_t capture_graph(const std::vector<gg_context*>& ctxs, cudaStream_t st, F&& f) {
+  cudaGraph_t g = nullptr;
+  GG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  for (auto* c : ctxs) c->capturing = true;
+  try {
+    f();
+  } catch (...) {
+    for (auto* c : ctxs) c->capturing = false;
+    cudaStreamEndCapture(st, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  for (auto* c : ctxs) c->capturing = false;
+  GG_CUDA(cudaStreamEndCapture(st, &g));
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) throw Error(GG_ERR_CUDA, std::string("graph instantiation: ") + cudaGetErrorString(e));
+  return ex;
+}
+
+extern "C" {
+
+// after a replay: the Dyson status recorded on the device and the split engine's flag
+static void graph_check(gg_context* c, int solver) {
+  int e[3] = {0, 0, 0};
+  GG_CUDA(cudaMemcpy(e, c->gw_err.p, sizeof(e), cudaMemcpyDeviceToHost));
+  if (c->split) split_check(c->split, c->stream);
+  if (e[0]) dyson_failure(c, solver, e[1], e[2]);
+}
+
+static void gw_device(gg_context* c, const double2* G, double2* Sigma, int solver, int precision, cudaStream_t st) {
+  if (!c->graph_mode || c->profiling || c->cap_P0 || c->cap_Pw || c->cap_Wt || st == nullptr) {
+    gw_sequence(c, G, Sigma, solver, precision, st);
+    return;
+  }
+  if (c->graph_exec && c->graph_G == G && c->graph_S == Sigma && c->graph_solver == solver &&
+      c->graph_prec == precision && c->graph_stream == st) {
+    GG_CUDA(cudaGraphLaunch(c->graph_exec, st));
+    GG_CUDA(cudaStreamSynchronize(st));
+    graph_check(c, solver);
+    return;
+  }
+  // eager build (allocates, builds the tables, gives this call's result), then capture the
+  // same sequence for the following calls
+  c->drop_graph();
+  gw_sequence(c, G, Sigma, solver, precision, st);
+  c->graph_exec = capture_graph({c}, st, [&] { gw_sequence(c, G, Sigma, solver, precision, st); });
+  c->graph_G = G;
+  c->graph_S = Sigma;
+  c->graph_solver = solver;
+  c->graph_prec = precision;
+  c->graph_stream = st;
+}
+
 // matrices per (outer, spin, k) block of a G / Sigma / dm buffer: nao^2 x ns, or (2 nao)^2 in X2C
 static size_t spin_elems(const gg_context* c) {
   const size_t nn = (size_t)c->sh.nao * c->sh.nao;
@@ -266,7 +333,121 @@ int gg_set_x2c(gg_context* c, int enable) {
   return guarded(c, [&] {
     if (enable && c->sh.ns != 1) throw Error(GG_ERR_ARG, "x2c: the spinor shape has ns = 1 (nso = 2 nao)");
     c->x2c = enable != 0;
+    c->invalidate();
   });
+}
+
+int gg_set_graph(gg_context* c, int enable) {
+  return guarded(c, [&] {
+    c->graph_mode = enable != 0;
+    c->drop_graph();
+  });
+}
+
+// several systems' GW builds in one CUDA graph, each on its own context stream
+struct gg_batch {
+  std::vector<gg_context*> ctx;
+  std::vector<const double2*> G;
+  std::vector<double2*> S;
+  int solver = 0, precision = 0;
+  cudaStream_t master = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t exec = nullptr;
+  ~gg_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    for (auto e : join) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (master) cudaStreamDestroy(master);
+  }
+};
+
+}  // extern "C"
+
+template <typename F>
+static int guarded_global(F&& f) {
+  try {
+    f();
+    return GG_OK;
+  } catch (const Error& e) {
+    gg::set_thread_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    gg::set_thread_error(e.what());
+    return GG_ERR_INTERNAL;
+  }
+}
+
+extern "C" {
+
+int gg_batch_create(gg_context* const* ctxs, int n, const void* const* G, void* const* Sigma, int solver,
+                    int precision, gg_batch** out) {
+  return guarded_global([&] {
+    if (!ctxs || n <= 0 || !G || !Sigma || !out) throw Error(GG_ERR_ARG, "batch: bad arguments");
+    *out = nullptr;
+    auto b = std::make_unique<gg_batch>();
+    const int dev = ctxs[0]->device;
+    GG_CUDA(cudaSetDevice(dev));
+    for (int i = 0; i < n; ++i) {
+      gg_context* c = ctxs[i];
+      if (!c || c->device != dev) throw Error(GG_ERR_ARG, "batch: contexts must exist and share one device");
+      if (c->profiling || c->cap_P0 || c->cap_Pw || c->cap_Wt)
+        throw Error(GG_ERR_STATE, "batch: profiling and intermediate capture need eager builds");
+      for (int j = 0; j < i; ++j)
+        if (ctxs[j] == c) throw Error(GG_ERR_ARG, "batch: a context appears twice");
+      b->ctx.push_back(c);
+      b->G.push_back((const double2*)G[i]);
+      b->S.push_back((double2*)Sigma[i]);
+    }
+    b->solver = solver;
+    b->precision = precision;
+    // eager builds: allocate every buffer and build every table, then capture all of them
+    for (int i = 0; i < n; ++i) {
+      try {
+        gw_sequence(b->ctx[i], b->G[i], b->S[i], solver, precision, b->ctx[i]->stream);
+      } catch (const Error& e) {
+        throw Error(e.code, "batch system " + std::to_string(i) + ": " + e.what());
+      }
+    }
+    GG_CUDA(cudaStreamCreateWithFlags(&b->master, cudaStreamNonBlocking));
+    GG_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    b->join.resize(n, nullptr);
+    for (int i = 0; i < n; ++i) GG_CUDA(cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming));
+    b->exec = capture_graph(b->ctx, b->master, [&] {
+      GG_CUDA(cudaEventRecord(b->fork, b->master));
+      for (int i = 0; i < n; ++i) {
+        cudaStream_t st = b->ctx[i]->stream;
+        GG_CUDA(cudaStreamWaitEvent(st, b->fork, 0));
+        gw_sequence(b->ctx[i], b->G[i], b->S[i], solver, precision, st);
+        GG_CUDA(cudaEventRecord(b->join[i], st));
+        GG_CUDA(cudaStreamWaitEvent(b->master, b->join[i], 0));
+      }
+    });
+    *out = b.release();
+  });
+}
+
+int gg_batch_run(gg_batch* b, void* stream) {
+  return guarded_global([&] {
+    if (!b) throw Error(GG_ERR_ARG, "batch: NULL");
+    GG_CUDA(cudaSetDevice(b->ctx[0]->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : b->master;
+    GG_CUDA(cudaGraphLaunch(b->exec, st));
+    GG_CUDA(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < b->ctx.size(); ++i) {
+      try {
+        graph_check(b->ctx[i], b->solver);
+      } catch (const Error& e) {
+        throw Error(e.code, "batch system " + std::to_string(i) + ": " + e.what());
+      }
+    }
+  });
+}
+
+void gg_batch_destroy(gg_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->ctx.empty() ? 0 : b->ctx[0]->device);
+  delete b;
 }
 
 int gg_gw_sigma_device(gg_context* c, const void* G, void* Sigma, int solver, int precision, void* stream) {

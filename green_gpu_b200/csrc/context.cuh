@@ -1,6 +1,7 @@
 // Per-system device state behind the opaque gg_context of the C ABI.
 #pragma once
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -109,7 +110,34 @@ struct gg_context {
 
   gg::SplitGemm* split = nullptr;
 
+  // tables of one GW build (pair positions and ops, G block indices), built on the first build
+  // after the symmetry, k-pairs or spin layout changed
+  std::shared_ptr<void> gw_tables;
+  // graph mode: the first build runs eagerly, the second is captured into a CUDA graph that
+  // later builds replay while inputs, buffers and settings match (any setter drops it)
+  bool graph_mode = false;
+  bool capturing = false;  // true while gw_build is being captured: no host syncs, no timers
+  cudaGraphExec_t graph_exec = nullptr;
+  const void* graph_G = nullptr;
+  void* graph_S = nullptr;
+  int graph_solver = -1, graph_prec = -1;
+  cudaStream_t graph_stream = nullptr;
+  gg::DevBuf<int> gw_err;  // [0] failed, [1] system index (q position x nw_b + Omega), [2] info
+  int plan_qc = 0, plan_kc = 0, plan_tb = 0;  // plan of the eager build, reused by the capture
+
+  void drop_graph() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+    graph_G = nullptr;
+    graph_S = nullptr;
+  }
+  void invalidate() {
+    gw_tables.reset();
+    drop_graph();
+  }
+
   ~gg_context() {
+    drop_graph();
     if (split) gg::split_release(split);
     if (stream) cudaStreamDestroy(stream);
   }

@@ -31,8 +31,10 @@ inline int64_t tri(long k1, long k2) { return k1 >= k2 ? k1 * (k1 + 1) / 2 + k2 
 struct EventTimer {
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
   cudaStream_t st;
-  explicit EventTimer(cudaStream_t s) : st(s) {}
+  bool on;
+  explicit EventTimer(cudaStream_t s, bool enabled = true) : st(s), on(enabled) {}
   int begin(int id) {
+    if (!on) return -1;
     cudaEvent_t a, b;
     GG_CUDA(cudaEventCreate(&a));
     GG_CUDA(cudaEventCreate(&b));
@@ -40,7 +42,9 @@ struct EventTimer {
     marks.push_back({id, {a, b}});
     return (int)marks.size() - 1;
   }
-  void end(int h) { GG_CUDA(cudaEventRecord(marks[h].second.second, st)); }
+  void end(int h) {
+    if (h >= 0) GG_CUDA(cudaEventRecord(marks[h].second.second, st));
+  }
   void collect(double* acc) {
     for (auto& m : marks) {
       float ms = 0;
@@ -83,6 +87,12 @@ struct IntTable {
     d.ensure(std::max<size_t>(h.size(), 1));
     if (!h.empty()) GG_CUDA(cudaMemcpy(d.p, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
   }
+};
+
+// tables of one GW build, kept in the context between builds
+struct GwTables {
+  PairTable p0_pairs, sg_pairs;
+  IntTable g1_idx;
 };
 
 size_t free_bytes() {
@@ -216,6 +226,18 @@ Plan plan_gw(gg_context* c, int slices) {
   return p;
 }
 
+// system index = position of q in this shard's list x nw_b + Omega
+void dyson_failure(const gg_context* c, int solver, int system, int info) {
+  const auto& s = c->sh;
+  const int nw = s.nw_b;
+  const int iq = c->shard_rank + (system / nw) * c->shard_size;
+  throw Error(solver == GG_SOLVER_CHOLESKY ? GG_ERR_NOT_HPD : GG_ERR_SINGULAR,
+              std::string(solver == GG_SOLVER_CHOLESKY ? "Cholesky" : "LU") + " failed for q_ibz " +
+                  std::to_string(iq) + ", frequency " + std::to_string(system % nw) + " (info " +
+                  std::to_string(info) + "): I - P~ is not " +
+                  (solver == GG_SOLVER_CHOLESKY ? "positive definite" : "invertible"));
+}
+
 void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solver, int precision, cudaStream_t st) {
   if (!c->has_sym || !c->has_kpairs || !c->V || !c->has_ir || c->sh.nw_b <= 0)
     throw Error(GG_ERR_STATE, "gw: symmetry, k-pairs, integrals and IR transforms (nw_b > 0) must be set first");
@@ -229,7 +251,22 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
   // (s1, s2) block of G^{k+q}(tau) with the (s2, s1) block of G^k(-tau), i.e. ab with ba
   // (copy_Gk_2c with minus_t = true, gw_gpu_kernel.cpp:523-536)
   auto spin_a = [&](int sp) { return (c->x2c && sp >= 2) ? 5 - sp : sp; };
-  const Plan pl = plan_gw(c, precision == GG_PREC_SPLIT ? c->slices : 0);
+  const bool cap = c->capturing;
+  Plan pl;
+  if (cap) {
+    // the captured build replays the eager build's chunking, so every buffer already exists
+    pl.qc = c->plan_qc;
+    pl.kc = c->plan_kc;
+    pl.tb = c->plan_tb;
+    pl.dyson_batch = 4 * 148;
+  } else {
+    pl = plan_gw(c, precision == GG_PREC_SPLIT ? c->slices : 0);
+    c->plan_qc = pl.qc;
+    c->plan_kc = pl.kc;
+    c->plan_tb = pl.tb;
+  }
+  if (cap && c->profiling) throw Error(GG_ERR_STATE, "gw: profiling is not available while capturing");
+  if (cap && (c->cap_P0 || c->cap_Pw || c->cap_Wt)) throw Error(GG_ERR_STATE, "gw: capture of intermediates needs an eager build");
   c->launches = 0;
 
   // work buffers (sized before the first launch)
@@ -289,16 +326,19 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
     }
   };
 
-  // pair tables: P0 pairs (k, k+q) for every irreducible q, Sigma pairs (k_ibz, k_ibz - q')
-  PairTable p0_pairs, sg_pairs;
-  {
+  // pair tables: P0 pairs (k, k+q) for every irreducible q, Sigma pairs (k_ibz, k_ibz - q');
+  // G1 block indices: block (k1 * ns + sp) of Gf, for every (iq, sp, k).  Built once per
+  // symmetry / k-pair / spin setting (the uploads synchronise, so never while capturing).
+  if (!c->gw_tables) {
+    if (cap) throw Error(GG_ERR_STATE, "gw: tables must be built by an eager build before capture");
+    auto tab = std::make_shared<GwTables>();
     std::vector<int> a, b;
     for (int iq = 0; iq < s.inq; ++iq)
       for (int k = 0; k < nk; ++k) {
         a.push_back(k);
         b.push_back((int)c->k1_from_k2q[(size_t)k * s.nq + c->q_r2f[iq]]);
       }
-    p0_pairs.build(c, a, b);
+    tab->p0_pairs.build(c, a, b);
     a.clear();
     b.clear();
     for (int qd = 0; qd < s.nq; ++qd)
@@ -307,19 +347,22 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
         a.push_back(k);
         b.push_back((int)c->k2_from_k1q[(size_t)k * s.nq + qd]);
       }
-    sg_pairs.build(c, a, b);
-  }
-  // G1 block indices: block (k1 * ns + sp) of Gf, for every (iq, sp, k)
-  IntTable g1_idx;
-  {
+    tab->sg_pairs.build(c, a, b);
     std::vector<int> v;
     for (int iq = 0; iq < s.inq; ++iq)
       for (int sp = 0; sp < ns; ++sp)
         for (int k = 0; k < nk; ++k) v.push_back((int)c->k1_from_k2q[(size_t)k * s.nq + c->q_r2f[iq]] * ns + sp);
-    g1_idx.build(v);
+    tab->g1_idx.build(v);
+    c->gw_tables = tab;
   }
+  const GwTables& tables = *std::static_pointer_cast<GwTables>(c->gw_tables);
+  const PairTable& p0_pairs = tables.p0_pairs;
+  const PairTable& sg_pairs = tables.sg_pairs;
+  const IntTable& g1_idx = tables.g1_idx;
+  int* gw_err = c->gw_err.ensure(4);
+  if (cap) GG_CUDA(cudaMemsetAsync(gw_err, 0, 4 * sizeof(int), st));
 
-  EventTimer tm(st);
+  EventTimer tm(st, !cap);
   int h_total = tm.begin(0);
   GG_CUDA(cudaMemsetAsync(Sigma_dev, 0, sizeof(double2) * (size_t)T * ns * s.ink * nn, st));
 
@@ -432,15 +475,16 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
       ++c->launches;
     }
     tm.end(h);
-    GG_CUDA(cudaMemcpyAsync(info_h.data(), info, sizeof(int) * qn * nw, cudaMemcpyDeviceToHost, st));
-    GG_CUDA(cudaStreamSynchronize(st));
-    for (int i = 0; i < qn * nw; ++i)
-      if (info_h[i] != 0)
-        throw Error(solver == GG_SOLVER_CHOLESKY ? GG_ERR_NOT_HPD : GG_ERR_SINGULAR,
-                    std::string(solver == GG_SOLVER_CHOLESKY ? "Cholesky" : "LU") + " failed for q_ibz " +
-                        std::to_string(myq[q0 + i / nw]) + ", frequency " + std::to_string(i % nw) + " (info " +
-                        std::to_string(info_h[i]) + "): I - P~ is not " +
-                        (solver == GG_SOLVER_CHOLESKY ? "positive definite" : "invertible"));
+    if (cap) {
+      // no host round trip inside a graph: the first failing system is recorded on the device
+      // and reported after the replay (dyson_failure)
+      launch_info_collect(info, qn * nw, q0 * nw, gw_err, st);
+    } else {
+      GG_CUDA(cudaMemcpyAsync(info_h.data(), info, sizeof(int) * qn * nw, cudaMemcpyDeviceToHost, st));
+      GG_CUDA(cudaStreamSynchronize(st));
+      for (int i = 0; i < qn * nw; ++i)
+        if (info_h[i] != 0) dyson_failure(c, solver, q0 * nw + i, info_h[i]);
+    }
     // ---------------- IR back: Wt[q][t] = sum_w Ttn[t][w] W[q][w]
     h = tm.begin(5);
     {
@@ -528,6 +572,7 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
     tm.end(h);
   }
   tm.end(h_total);
+  if (cap) return;  // the caller checks gw_err and the split engine's flag after the replay
   GG_CUDA(cudaStreamSynchronize(st));
   if (split) split_check(split, st);
   for (auto& e : kev) {

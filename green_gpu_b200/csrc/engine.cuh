@@ -12,6 +12,8 @@ int hf_spins(const gg_context* c);
 // X2C needs the identity k/q symmetry (no rotations, no time-reversal partners): the spinor
 // transformation of G under a space-group or time-reversal operation is not applied here
 void x2c_check(const gg_context* c);
+// throws the Dyson failure of `system` (q position in the shard x nw_b + Omega)
+void dyson_failure(const gg_context* c, int solver, int system, int info);
 void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solver, int precision, cudaStream_t st);
 void hf_exchange(gg_context* c, const double2* dm_dev, double2* K_dev, cudaStream_t st);
 void hf_direct(gg_context* c, double2* F_dev, cudaStream_t st);

@@ -554,6 +554,21 @@ void launch_x2c_merge(const double2* in, long nouter, long ninner, int n, int nb
   GG_CHECK_LAUNCH();
 }
 
+namespace {
+__global__ void info_collect_kernel(const int* info, int count, int base, int* err) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    if (info[i] != 0 && atomicCAS(&err[0], 0, 1) == 0) {
+      err[1] = base + i;
+      err[2] = info[i];
+    }
+}
+}  // namespace
+
+void launch_info_collect(const int* info, int count, int base, int* err, cudaStream_t st) {
+  info_collect_kernel<<<grid_for(count), TPB, 0, st>>>(info, count, base, err);
+  GG_CHECK_LAUNCH();
+}
+
 void launch_axpy(double2* y, const double2* x, long n, cudaStream_t st) {
   axpy_kernel<<<grid_for(n), TPB, 0, st>>>(y, x, n);
   GG_CHECK_LAUNCH();

@@ -23,6 +23,8 @@ void launch_gather_blocks(const double2* src, const int* idx_d, int nblocks, lon
                           double2* out, cudaStream_t st);
 // y += x (n complex numbers)
 void launch_axpy(double2* y, const double2* x, long n, cudaStream_t st);
+// err[0..2] <- (1, base + i, info[i]) for a failing system i (info != 0), if none is recorded yet
+void launch_info_collect(const int* info, int count, int base, int* err, cudaStream_t st);
 
 // Two-component (X2C) spin blocks.  A spinor matrix of order 2n holds the blocks aa (0,0),
 // bb (n,n), ab (0,n) and ba (n,0).  Block ss of the pseudo-spin order is (row, col) =

@@ -31,7 +31,8 @@ EXPORTS = [
     "gg_set_coulomb_device", "gg_set_ir", "gg_set_split_slices", "gg_gw_sigma", "gg_gw_sigma_device",
     "gg_set_capture", "gg_hf_exchange", "gg_hf_fock", "gg_symmetry_unfold", "gg_last_timings", "gg_version",
     "gg_set_profiling", "gg_kernel_stats", "gg_last_launch_count", "gg_set_q_shard", "gg_zgemm",
-    "gg_zgemm_noalloc", "gg_set_hf_precision", "gg_estimate_bytes", "gg_set_x2c",
+    "gg_zgemm_noalloc", "gg_set_hf_precision", "gg_estimate_bytes", "gg_set_x2c", "gg_set_graph",
+    "gg_batch_create", "gg_batch_run", "gg_batch_destroy",
 ]
 
 
@@ -85,6 +86,11 @@ def load(path: str = LIB_PATH):
         "gg_zgemm_noalloc": (C.c_int, [C.c_int64, C.c_int64, C.c_int64, P, P, P, P]),
         "gg_set_hf_precision": (C.c_int, [P, C.c_int]),
         "gg_set_x2c": (C.c_int, [P, C.c_int]),
+        "gg_set_graph": (C.c_int, [P, C.c_int]),
+        "gg_batch_create": (C.c_int, [C.POINTER(P), C.c_int, C.POINTER(P), C.POINTER(P), C.c_int, C.c_int,
+                                      C.POINTER(P)]),
+        "gg_batch_run": (C.c_int, [P, P]),
+        "gg_batch_destroy": (None, [P]),
         "gg_estimate_bytes": (C.c_int, [C.POINTER(Shape), C.c_int64, C.POINTER(C.c_int64)]),
     }
     for name, (res, args) in sig.items():
@@ -179,6 +185,10 @@ class Context:
         """Two-component mode: G / Sigma / dm / S_k / Fock are spinor matrices of order 2 nao."""
         self._check(self.lib.gg_set_x2c(self.h, int(bool(enable))))
         self.x2c = bool(enable)
+
+    def set_graph(self, enable: bool = True):
+        """Capture the GW build into a CUDA graph after its first eager run and replay it."""
+        self._check(self.lib.gg_set_graph(self.h, int(bool(enable))))
 
     def _mat(self):
         """(spin blocks, matrix order) of the caller's G / dm layout."""
@@ -297,3 +307,40 @@ def context_for(sys_, device=0, upload_V=True) -> Context:
     if sys_.nw_b > 0 and sys_.Ttn_FB.size:
         ctx.set_ir(sys_.Ttn_FB, sys_.Tnt_BF)
     return ctx
+
+
+class Batch:
+    """Several systems' GW builds in one CUDA graph (gg_batch_create / gg_batch_run).
+
+    ``items`` are (Context, G_device_ptr, Sigma_device_ptr) triples; creating the batch runs each
+    build once eagerly, ``run()`` replays all of them."""
+
+    def __init__(self, items, solver=SOLVER_CHOLESKY, precision=PREC_FP64):
+        self.lib = load()
+        n = len(items)
+        P = C.c_void_p
+        ctxs = (P * n)(*[it[0].h for it in items])
+        gs = (P * n)(*[int(it[1]) for it in items])
+        ss = (P * n)(*[int(it[2]) for it in items])
+        self._keep = items
+        h = P()
+        rc = self.lib.gg_batch_create(ctxs, n, gs, ss, int(solver), int(precision), C.byref(h))
+        if rc != GG_OK:
+            raise GreenError(rc, self.lib.gg_last_error(None).decode())
+        self.h = h
+
+    def run(self, stream=0):
+        rc = self.lib.gg_batch_run(self.h, C.c_void_p(int(stream)))
+        if rc != GG_OK:
+            raise GreenError(rc, self.lib.gg_last_error(None).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.gg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

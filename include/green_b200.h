@@ -146,6 +146,26 @@ int gg_set_hf_precision(gg_context* ctx, int precision);
  * with S_aa.  Only the identity k/q symmetry is accepted (GG_ERR_ARG otherwise). */
 int gg_set_x2c(gg_context* ctx, int enable);
 
+/* Graph mode for gg_gw_sigma / gg_gw_sigma_device (no counterpart in the reference, which
+ * launches every contraction from the host: cugw_utils.cu:104-202).  With graph mode on, the
+ * first build runs eagerly and is then captured into one CUDA graph; later builds with the same
+ * buffers, stream, solver and precision replay it (one launch instead of tens of thousands).
+ * Dyson failures and split-engine time-outs are still reported, after the replay.  Every setter
+ * of the context drops the graph; profiling and intermediate capture fall back to eager builds. */
+int gg_set_graph(gg_context* ctx, int enable);
+
+/* Several systems (contexts of any shape on one device) built in one CUDA graph: each system's
+ * build runs on its own context stream, so their kernels overlap on the device.
+ * gg_batch_create runs every build once eagerly (the results are valid) and captures them;
+ * gg_batch_run replays all of them (stream NULL: the batch's own stream) and returns the first
+ * failure (message through gg_last_error(NULL)).  G[i] / Sigma[i] are device buffers of system i
+ * in its layout; the contexts must not be changed while the batch exists. */
+typedef struct gg_batch gg_batch;
+int gg_batch_create(gg_context* const* ctxs, int n, const void* const* G_device, void* const* Sigma_device,
+                    int solver, int precision, gg_batch** out);
+int gg_batch_run(gg_batch* batch, void* stream);
+void gg_batch_destroy(gg_batch* batch);
+
 /* Exchange part K_s(k) [ns][ink][nao][nao] for the IBZ density dm [ns][ink][nao][nao]
  * (host buffers). */
 int gg_hf_exchange(gg_context* ctx, const double* dm, double* K_out);
