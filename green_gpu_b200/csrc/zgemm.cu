@@ -41,8 +41,13 @@ __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-template <bool A_K, bool B_K>
-__global__ void __launch_bounds__(NT, 2) zgemm_kernel(ZgemmDesc d, int tiles_m, int tiles_n) {
+// One CTA computes a run of `span` consecutive tiles along M (span_m) or N, so that for short
+// reductions the cp.async ring runs on across tile boundaries: the next tile's first stages
+// load while the current tile's epilogue stores (span = 1: one tile per CTA).
+template <bool A_K, bool B_K, bool SPAN>
+__global__ void __launch_bounds__(NT, 2)
+    zgemm_kernel(ZgemmDesc d, int tiles_m, int tiles_n, int span, int span_m) {
+  if (!SPAN) span = 1;
   __shared__ __align__(16) double2 As[STAGES][TILE];
   __shared__ __align__(16) double2 Bs[STAGES][TILE];
 
@@ -51,17 +56,21 @@ __global__ void __launch_bounds__(NT, 2) zgemm_kernel(ZgemmDesc d, int tiles_m, 
   const int warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1;
 
+  // grid: groups of `span` tiles along the spanned dimension
+  const int groups_m = span_m ? (tiles_m + span - 1) / span : tiles_m;
+  const int groups_n = span_m ? tiles_n : (tiles_n + span - 1) / span;
   const long bid = blockIdx.x;
-  const int ntile = tiles_m * tiles_n;
-  const int tile = (int)(bid % ntile);
-  const long rest = bid / ntile;
+  const int ngroup = groups_m * groups_n;
+  const int group = (int)(bid % ngroup);
+  const long rest = bid / ngroup;
   const int split = (int)(rest % d.splits);
   const long batch = rest / d.splits;
   const int b0 = (int)(batch % d.nb0);
   const int b1 = (int)((batch / d.nb0) % d.nb1);
   const int b2 = (int)(batch / ((long)d.nb0 * d.nb1));
-  const int tm = tile % tiles_m, tn = tile / tiles_m;
-  const int m0 = tm * BM, n0 = tn * BN;
+  const int gm = group % groups_m, gn = group / groups_m;
+  const int tm0 = span_m ? gm * span : gm, tn0 = span_m ? gn : gn * span;
+  const int ntiles = !SPAN ? 1 : span_m ? min(span, tiles_m - tm0) : min(span, tiles_n - tn0);
 
   const double2* Ab = d.A + b0 * d.a_b0 + b1 * d.a_b1 + b2 * d.a_b2;
   const double2* Bb = d.B + b0 * d.b_b0 + b1 * d.b_b1 + b2 * d.b_b2;
@@ -71,22 +80,30 @@ __global__ void __launch_bounds__(NT, 2) zgemm_kernel(ZgemmDesc d, int tiles_m, 
   //   !KMAJ: row = tid % 64, k = tid / 64 + 2 i
   long a_off[4], b_off[4];
   bool a_ok[4], b_ok[4];
+  auto set_a = [&](int m0) {
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int ra = A_K ? tid / 8 + 16 * i : tid % 64;
-    const int m = m0 + ra;
-    a_ok[i] = m < d.M;
-    a_off[i] = a_ok[i] ? d.a_m(m) : 0;
-    const int rb = B_K ? tid / 8 + 16 * i : tid % 64;
-    const int n = n0 + rb;
-    b_ok[i] = n < d.N;
-    b_off[i] = b_ok[i] ? d.b_n(n) : 0;
-  }
+    for (int i = 0; i < 4; ++i) {
+      const int m = m0 + (A_K ? tid / 8 + 16 * i : tid % 64);
+      a_ok[i] = m < d.M;
+      a_off[i] = a_ok[i] ? d.a_m(m) : 0;
+    }
+  };
+  auto set_b = [&](int n0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int n = n0 + (B_K ? tid / 8 + 16 * i : tid % 64);
+      b_ok[i] = n < d.N;
+      b_off[i] = b_ok[i] ? d.b_n(n) : 0;
+    }
+  };
+  set_a(tm0 * BM);
+  set_b(tn0 * BN);
 
   const int ktiles = (d.K + BK - 1) / BK;
   const long total = (long)d.KB * ktiles;
   const long t_begin = total * split / d.splits;
   const long t_end = total * (split + 1) / d.splits;
+  const long per_tile = t_end - t_begin;
 
   auto issue = [&](long t, int st) {
     const int kb = (int)(t / ktiles);
@@ -110,96 +127,172 @@ __global__ void __launch_bounds__(NT, 2) zgemm_kernel(ZgemmDesc d, int tiles_m, 
       cp_async16(&Bs[st][sidx<B_K>(r, kk)], v ? (const void*)(Bk + b_off[i] + k * d.b_k) : (const void*)Bb, v);
     }
   };
+  // issue stream over the run of tiles: (itile, it) is the next step to load
+  int itile = 0;
+  long it = t_begin;
+  auto issue_next = [&](int st) {
+    if (itile >= ntiles) return;
+    issue(it, st);
+    if (++it == t_end) {
+      it = t_begin;
+      if (++itile < ntiles) {
+        if (span_m) set_a((tm0 + itile) * BM);
+        else set_b((tn0 + itile) * BN);
+      }
+    }
+  };
 
   double cr[4][4][2], ci[4][4][2];
+  auto zero_acc = [&]() {
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      cr[a][b][0] = cr[a][b][1] = 0.0;
-      ci[a][b][0] = ci[a][b][1] = 0.0;
-    }
+      for (int b = 0; b < 4; ++b) {
+        cr[a][b][0] = cr[a][b][1] = 0.0;
+        ci[a][b][0] = ci[a][b][1] = 0.0;
+      }
+  };
+  zero_acc();
 
   const double sa = d.conjA ? -1.0 : 1.0;
   const double sb = d.conjB ? -1.0 : 1.0;
   const int fr = lane >> 2, fk = lane & 3;
 
-  // prologue: STAGES-1 tiles in flight
+  auto epilogue = [&](int m0, int n0) {
+    const long batch_count = (long)d.nb0 * d.nb1 * d.nb2;
+    const double2* cbase = d.C + b0 * d.c_b0 + b1 * d.c_b1 + b2 * d.c_b2;
+    const bool use_beta = d.beta.x != 0.0 || d.beta.y != 0.0;
 #pragma unroll
-  for (int s = 0; s < STAGES - 1; ++s) {
-    if (t_begin + s < t_end) issue(t_begin + s, s);
-    cp_commit();
-  }
-  int st = 0;
-  for (long t = t_begin; t < t_end; ++t) {
-    cp_wait<STAGES - 2>();
-    __syncthreads();
-    // refill the stage consumed in the previous iteration
-    {
-      const long tn_ = t + STAGES - 1;
-      int sn = st + STAGES - 1;
-      if (sn >= STAGES) sn -= STAGES;
-      if (tn_ < t_end) issue(tn_, sn);
-      cp_commit();
-    }
-    const double2* as = As[st];
-    const double2* bs = Bs[st];
-#pragma unroll
-    for (int ks = 0; ks < BK / 4; ++ks) {
-      double ar[4], ai[4], an[4], br[4], bi[4];
-#pragma unroll
-      for (int mt = 0; mt < 4; ++mt) {
-        const double2 v = as[sidx<A_K>(wm * 32 + mt * 8 + fr, ks * 4 + fk)];
-        ar[mt] = v.x;
-        ai[mt] = sa * v.y;
-        an[mt] = -ai[mt];
-      }
+    for (int mt = 0; mt < 4; ++mt) {
+      const int m = m0 + wm * 32 + mt * 8 + fr;
+      if (m >= d.M) continue;
+      const long cm = d.c_m(m);
 #pragma unroll
       for (int nt = 0; nt < 4; ++nt) {
-        const double2 v = bs[sidx<B_K>(wn * 32 + nt * 8 + fr, ks * 4 + fk)];
-        br[nt] = v.x;
-        bi[nt] = sb * v.y;
-      }
 #pragma unroll
-      for (int mt = 0; mt < 4; ++mt)
+        for (int j = 0; j < 2; ++j) {
+          const int n = n0 + wn * 32 + nt * 8 + 2 * fk + j;
+          if (n >= d.N) continue;
+          const double2 acc = make_double2(cr[mt][nt][j], ci[mt][nt][j]);
+          if (d.splits > 1) {
+            d.work[((split * batch_count + batch) * d.M + m) * (long)d.N + n] = acc;
+          } else {
+            double2* c = const_cast<double2*>(cbase) + cm + d.c_n(n);
+            double2 v = cmul(d.alpha, acc);
+            if (use_beta) v = cadd(v, cmul(d.beta, *c));
+            *c = v;
+          }
+        }
+      }
+    }
+  };
+
+  int st = 0;
+  if constexpr (SPAN) {
+    // prologue: STAGES-1 stages in flight (possibly reaching into the next tiles)
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+      issue_next(s);
+      cp_commit();
+    }
+    int ctile = 0;   // tile being computed
+    long cstep = 0;  // its step
+    const long steps = (long)ntiles * per_tile;
+    for (long s = 0; s < steps; ++s) {
+      cp_wait<STAGES - 2>();
+      __syncthreads();
+      {
+        int sn = st + STAGES - 1;
+        if (sn >= STAGES) sn -= STAGES;
+        issue_next(sn);
+        cp_commit();
+      }
+      const double2* as = As[st];
+      const double2* bs = Bs[st];
+#pragma unroll
+      for (int ks = 0; ks < BK / 4; ++ks) {
+        double ar[4], ai[4], an[4], br[4], bi[4];
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) {
+          const double2 v = as[sidx<A_K>(wm * 32 + mt * 8 + fr, ks * 4 + fk)];
+          ar[mt] = v.x;
+          ai[mt] = sa * v.y;
+          an[mt] = -ai[mt];
+        }
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
-          dmma(cr[mt][nt][0], cr[mt][nt][1], ar[mt], br[nt]);
-          dmma(cr[mt][nt][0], cr[mt][nt][1], an[mt], bi[nt]);
-          dmma(ci[mt][nt][0], ci[mt][nt][1], ar[mt], bi[nt]);
-          dmma(ci[mt][nt][0], ci[mt][nt][1], ai[mt], br[nt]);
+          const double2 v = bs[sidx<B_K>(wn * 32 + nt * 8 + fr, ks * 4 + fk)];
+          br[nt] = v.x;
+          bi[nt] = sb * v.y;
         }
-    }
-    st = (st + 1 == STAGES) ? 0 : st + 1;
-  }
-  cp_wait<0>();
-
-  // epilogue
-  const long batch_count = (long)d.nb0 * d.nb1 * d.nb2;
-  const double2* cbase = d.C + b0 * d.c_b0 + b1 * d.c_b1 + b2 * d.c_b2;
-  const bool use_beta = d.beta.x != 0.0 || d.beta.y != 0.0;
 #pragma unroll
-  for (int mt = 0; mt < 4; ++mt) {
-    const int m = m0 + wm * 32 + mt * 8 + fr;
-    if (m >= d.M) continue;
-    const long cm = d.c_m(m);
+        for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-    for (int nt = 0; nt < 4; ++nt) {
-#pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const int n = n0 + wn * 32 + nt * 8 + 2 * fk + j;
-        if (n >= d.N) continue;
-        const double2 acc = make_double2(cr[mt][nt][j], ci[mt][nt][j]);
-        if (d.splits > 1) {
-          d.work[((split * batch_count + batch) * d.M + m) * (long)d.N + n] = acc;
-        } else {
-          double2* c = const_cast<double2*>(cbase) + cm + d.c_n(n);
-          double2 v = cmul(d.alpha, acc);
-          if (use_beta) v = cadd(v, cmul(d.beta, *c));
-          *c = v;
-        }
+          for (int nt = 0; nt < 4; ++nt) {
+            dmma(cr[mt][nt][0], cr[mt][nt][1], ar[mt], br[nt]);
+            dmma(cr[mt][nt][0], cr[mt][nt][1], an[mt], bi[nt]);
+            dmma(ci[mt][nt][0], ci[mt][nt][1], ar[mt], bi[nt]);
+            dmma(ci[mt][nt][0], ci[mt][nt][1], ai[mt], br[nt]);
+          }
+      }
+      st = (st + 1 == STAGES) ? 0 : st + 1;
+      if (++cstep == per_tile) {
+        epilogue((tm0 + (span_m ? ctile : 0)) * BM, (tn0 + (span_m ? 0 : ctile)) * BN);
+        zero_acc();
+        cstep = 0;
+        ++ctile;
       }
     }
+    cp_wait<0>();
+  } else {
+    // one tile: prologue of STAGES-1 stages, then refill one stage per step
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+      if (t_begin + s < t_end) issue(t_begin + s, s);
+      cp_commit();
+    }
+    for (long t = t_begin; t < t_end; ++t) {
+      cp_wait<STAGES - 2>();
+      __syncthreads();
+      {
+        const long tn_ = t + STAGES - 1;
+        int sn = st + STAGES - 1;
+        if (sn >= STAGES) sn -= STAGES;
+        if (tn_ < t_end) issue(tn_, sn);
+        cp_commit();
+      }
+      const double2* as = As[st];
+      const double2* bs = Bs[st];
+#pragma unroll
+      for (int ks = 0; ks < BK / 4; ++ks) {
+        double ar[4], ai[4], an[4], br[4], bi[4];
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) {
+          const double2 v = as[sidx<A_K>(wm * 32 + mt * 8 + fr, ks * 4 + fk)];
+          ar[mt] = v.x;
+          ai[mt] = sa * v.y;
+          an[mt] = -ai[mt];
+        }
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          const double2 v = bs[sidx<B_K>(wn * 32 + nt * 8 + fr, ks * 4 + fk)];
+          br[nt] = v.x;
+          bi[nt] = sb * v.y;
+        }
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt) {
+            dmma(cr[mt][nt][0], cr[mt][nt][1], ar[mt], br[nt]);
+            dmma(cr[mt][nt][0], cr[mt][nt][1], an[mt], bi[nt]);
+            dmma(ci[mt][nt][0], ci[mt][nt][1], ar[mt], bi[nt]);
+            dmma(ci[mt][nt][0], ci[mt][nt][1], ai[mt], br[nt]);
+          }
+      }
+      st = (st + 1 == STAGES) ? 0 : st + 1;
+    }
+    cp_wait<0>();
+    epilogue(tm0 * BM, tn0 * BN);
   }
 }
 
@@ -226,8 +319,11 @@ __global__ void zgemm_reduce(ZgemmDesc d) {
 }
 
 template <bool A_K, bool B_K>
-void launch(const ZgemmDesc& d, int tiles_m, int tiles_n, long blocks, cudaStream_t stream) {
-  zgemm_kernel<A_K, B_K><<<(unsigned)blocks, NT, 0, stream>>>(d, tiles_m, tiles_n);
+void launch(const ZgemmDesc& d, int tiles_m, int tiles_n, int span, int span_m, long blocks, cudaStream_t stream) {
+  if (span > 1)
+    zgemm_kernel<A_K, B_K, true><<<(unsigned)blocks, NT, 0, stream>>>(d, tiles_m, tiles_n, span, span_m);
+  else
+    zgemm_kernel<A_K, B_K, false><<<(unsigned)blocks, NT, 0, stream>>>(d, tiles_m, tiles_n, 1, 0);
   GG_CHECK_LAUNCH();
 }
 
@@ -271,13 +367,29 @@ int zgemm(const ZgemmDesc& d0, cudaStream_t stream) {
     }
   }
   d.splits = splits;
-  const long blocks = base * splits;
+  // short reductions: runs of up to 4 tiles per CTA along the longer tile dimension, as long
+  // as at least 8 waves of CTAs remain (the ring then overlaps a tile's epilogue with the next
+  // tile's first loads)
+  int span = 1, span_m = 0;
+  if (splits == 1 && ksteps <= 16) {
+    span_m = tiles_m >= tiles_n ? 1 : 0;
+    const int along = span_m ? tiles_m : tiles_n;
+    const long other = base / along;
+    for (int sp = 4; sp >= 2; --sp)
+      if (along >= sp && other * ((along + sp - 1) / sp) >= 8 * slots) {
+        span = sp;
+        break;
+      }
+  }
+  const long groups = span_m ? (long)((tiles_m + span - 1) / span) * tiles_n * batch
+                             : (long)tiles_m * ((tiles_n + span - 1) / span) * batch;
+  const long blocks = groups * splits;
   if (blocks > 0x7fffffffL) throw Error(GG_ERR_ARG, "zgemm: grid too large");
   const bool ak = (d.a_k == 1), bk = (d.b_k == 1);
-  if (ak && bk) launch<true, true>(d, tiles_m, tiles_n, blocks, stream);
-  else if (ak) launch<true, false>(d, tiles_m, tiles_n, blocks, stream);
-  else if (bk) launch<false, true>(d, tiles_m, tiles_n, blocks, stream);
-  else launch<false, false>(d, tiles_m, tiles_n, blocks, stream);
+  if (ak && bk) launch<true, true>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  else if (ak) launch<true, false>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  else if (bk) launch<false, true>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  else launch<false, false>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
   int launches = 1;
   if (splits > 1) {
     const long total = (long)d.M * d.N * batch;

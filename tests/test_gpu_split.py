@@ -70,3 +70,14 @@ def test_gw_split_matches_oracle(S):
     out = c.gw_sigma(s.G_tskij, precision=native.PREC_SPLIT)
     ref = ogw.gw_build(s)
     assert rel(out, ref) < {4: 1e-6, 6: 1e-9}[S]
+
+
+@pytest.mark.parametrize("M,N", [(6400, 3072), (2560, 16000)])
+def test_fp64_zgemm_tile_runs_match_numpy(ctx, M, N):
+    # short reductions (K = 52) over many tiles take the path where one CTA computes a run of
+    # consecutive tiles along M (first case) or N (second, with a partial last run)
+    rng = np.random.default_rng(M + N)
+    K = 52
+    A = rng.standard_normal((M, K)) + 1j * rng.standard_normal((M, K))
+    B = rng.standard_normal((K, N)) + 1j * rng.standard_normal((K, N))
+    assert rel(ctx.zgemm(A, B), A @ B) < 1e-14
