@@ -226,14 +226,23 @@ __global__ void __launch_bounds__(NT, 2)
           bi[nt] = sb * v.y;
         }
 #pragma unroll
+        // four passes over the 16 accumulator tiles: consecutive DMMAs never share an
+        // accumulator, so each waits on a result issued 16 instructions earlier
         for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-          for (int nt = 0; nt < 4; ++nt) {
-            dmma(cr[mt][nt][0], cr[mt][nt][1], ar[mt], br[nt]);
-            dmma(cr[mt][nt][0], cr[mt][nt][1], an[mt], bi[nt]);
-            dmma(ci[mt][nt][0], ci[mt][nt][1], ar[mt], bi[nt]);
-            dmma(ci[mt][nt][0], ci[mt][nt][1], ai[mt], br[nt]);
-          }
+          for (int nt = 0; nt < 4; ++nt) dmma(cr[mt][nt][0], cr[mt][nt][1], ar[mt], br[nt]);
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt) dmma(ci[mt][nt][0], ci[mt][nt][1], ar[mt], bi[nt]);
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt) dmma(cr[mt][nt][0], cr[mt][nt][1], an[mt], bi[nt]);
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt) dmma(ci[mt][nt][0], ci[mt][nt][1], ai[mt], br[nt]);
       }
       st = (st + 1 == STAGES) ? 0 : st + 1;
       if (++cstep == per_tile) {
@@ -280,14 +289,23 @@ __global__ void __launch_bounds__(NT, 2)
           bi[nt] = sb * v.y;
         }
 #pragma unroll
+        // four passes over the 16 accumulator tiles: consecutive DMMAs never share an
+        // accumulator, so each waits on a result issued 16 instructions earlier
         for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-          for (int nt = 0; nt < 4; ++nt) {
-            dmma(cr[mt][nt][0], cr[mt][nt][1], ar[mt], br[nt]);
-            dmma(cr[mt][nt][0], cr[mt][nt][1], an[mt], bi[nt]);
-            dmma(ci[mt][nt][0], ci[mt][nt][1], ar[mt], bi[nt]);
-            dmma(ci[mt][nt][0], ci[mt][nt][1], ai[mt], br[nt]);
-          }
+          for (int nt = 0; nt < 4; ++nt) dmma(cr[mt][nt][0], cr[mt][nt][1], ar[mt], br[nt]);
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt) dmma(ci[mt][nt][0], ci[mt][nt][1], ar[mt], bi[nt]);
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt) dmma(cr[mt][nt][0], cr[mt][nt][1], an[mt], bi[nt]);
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt) dmma(ci[mt][nt][0], ci[mt][nt][1], ai[mt], br[nt]);
       }
       st = (st + 1 == STAGES) ? 0 : st + 1;
     }
