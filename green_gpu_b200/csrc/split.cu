@@ -21,7 +21,8 @@
 // the long reductions of the polarization contraction leaves DRAM pages mostly unused).
 //
 // Kernel roles (one CTA per SM, 320 threads): warp 0 issues TMA loads (3D tensor maps over
-// the planes, 64-byte swizzle, no multicast) of all S slices of an A and a B K-block into a
+// the planes, 64-byte swizzle, each CTA loading only for itself) of all S slices of an A
+// and a B K-block into a
 // ring; warp 1 owns TMEM and issues tcgen05.mma from one thread; warps 2..9 drain TMEM
 // with tcgen05.ld.  Every mbarrier wait is bounded: on time-out the kernel records an error
 // code, stops issuing work, waits (bounded) for what it already issued and frees TMEM.
