@@ -290,9 +290,12 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
   SplitGemm* split = nullptr;
   if (precision == GG_PREC_SPLIT) split = split_engine(c);
 
+  // FP64 contractions of a split-precision build use the three-product complex form
+  // (error ~1e-16 relative, far inside that build's budget)
   auto gemm = [&](ZgemmDesc d) {
     d.work = gw_work;
     d.work_elems = (long)c->gemm_work.n;
+    d.gauss = split ? 1 : 0;
     c->launches += zgemm(d, st);
   };
   // the dominant contractions go through the split-precision engine when requested;

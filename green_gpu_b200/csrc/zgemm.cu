@@ -1,6 +1,7 @@
 // Batched complex FP64 GEMM engine (see zgemm.cuh).
 //
-// CTA tile 64 x 64 complex, K step 8 complex, 4 warps in a 2 x 2 layout, each warp a
+// Two kernels share the tile, the staging and the grid.  The four-warp kernel: CTA tile
+// 64 x 64 complex, K step 8 complex, 4 warps in a 2 x 2 layout, each warp a
 // 32 x 32 complex tile = 4 x 4 DMMA 8x8 tiles per real/imag plane.  Complex products use
 // four real DMMAs (rr, -ii, ri, ir) on fragments read with one 16-byte shared load each
 // (interleaved complex in shared memory).  Global->shared staging uses cp.async (16 B,
@@ -41,13 +42,10 @@ __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-// One CTA computes a run of `span` consecutive tiles along M (span_m) or N, so that for short
-// reductions the cp.async ring runs on across tile boundaries: the next tile's first stages
-// load while the current tile's epilogue stores (span = 1: one tile per CTA).
-template <bool A_K, bool B_K, bool SPAN>
+// One CTA per (tile, split, batch entry) for reductions of any length.
+template <bool A_K, bool B_K>
 __global__ void __launch_bounds__(NT, 2)
-    zgemm_kernel(ZgemmDesc d, int tiles_m, int tiles_n, int span, int span_m) {
-  if (!SPAN) span = 1;
+    zgemm_kernel(ZgemmDesc d, int tiles_m, int tiles_n) {
   __shared__ __align__(16) double2 As[STAGES][TILE];
   __shared__ __align__(16) double2 Bs[STAGES][TILE];
 
@@ -56,21 +54,16 @@ __global__ void __launch_bounds__(NT, 2)
   const int warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1;
 
-  // grid: groups of `span` tiles along the spanned dimension
-  const int groups_m = span_m ? (tiles_m + span - 1) / span : tiles_m;
-  const int groups_n = span_m ? tiles_n : (tiles_n + span - 1) / span;
   const long bid = blockIdx.x;
-  const int ngroup = groups_m * groups_n;
-  const int group = (int)(bid % ngroup);
-  const long rest = bid / ngroup;
+  const int ntile = tiles_m * tiles_n;
+  const int tile = (int)(bid % ntile);
+  const long rest = bid / ntile;
   const int split = (int)(rest % d.splits);
   const long batch = rest / d.splits;
   const int b0 = (int)(batch % d.nb0);
   const int b1 = (int)((batch / d.nb0) % d.nb1);
   const int b2 = (int)(batch / ((long)d.nb0 * d.nb1));
-  const int gm = group % groups_m, gn = group / groups_m;
-  const int tm0 = span_m ? gm * span : gm, tn0 = span_m ? gn : gn * span;
-  const int ntiles = !SPAN ? 1 : span_m ? min(span, tiles_m - tm0) : min(span, tiles_n - tn0);
+  const int tm0 = tile % tiles_m, tn0 = tile / tiles_m;
 
   const double2* Ab = d.A + b0 * d.a_b0 + b1 * d.a_b1 + b2 * d.a_b2;
   const double2* Bb = d.B + b0 * d.b_b0 + b1 * d.b_b1 + b2 * d.b_b2;
@@ -103,7 +96,6 @@ __global__ void __launch_bounds__(NT, 2)
   const long total = (long)d.KB * ktiles;
   const long t_begin = total * split / d.splits;
   const long t_end = total * (split + 1) / d.splits;
-  const long per_tile = t_end - t_begin;
 
   auto issue = [&](long t, int st) {
     const int kb = (int)(t / ktiles);
@@ -127,21 +119,6 @@ __global__ void __launch_bounds__(NT, 2)
       cp_async16(&Bs[st][sidx<B_K>(r, kk)], v ? (const void*)(Bk + b_off[i] + k * d.b_k) : (const void*)Bb, v);
     }
   };
-  // issue stream over the run of tiles: (itile, it) is the next step to load
-  int itile = 0;
-  long it = t_begin;
-  auto issue_next = [&](int st) {
-    if (itile >= ntiles) return;
-    issue(it, st);
-    if (++it == t_end) {
-      it = t_begin;
-      if (++itile < ntiles) {
-        if (span_m) set_a((tm0 + itile) * BM);
-        else set_b((tn0 + itile) * BN);
-      }
-    }
-  };
-
   double cr[4][4][2], ci[4][4][2];
   auto zero_acc = [&]() {
 #pragma unroll
@@ -188,73 +165,8 @@ __global__ void __launch_bounds__(NT, 2)
   };
 
   int st = 0;
-  if constexpr (SPAN) {
-    // prologue: STAGES-1 stages in flight (possibly reaching into the next tiles)
-#pragma unroll
-    for (int s = 0; s < STAGES - 1; ++s) {
-      issue_next(s);
-      cp_commit();
-    }
-    int ctile = 0;   // tile being computed
-    long cstep = 0;  // its step
-    const long steps = (long)ntiles * per_tile;
-    for (long s = 0; s < steps; ++s) {
-      cp_wait<STAGES - 2>();
-      __syncthreads();
-      {
-        int sn = st + STAGES - 1;
-        if (sn >= STAGES) sn -= STAGES;
-        issue_next(sn);
-        cp_commit();
-      }
-      const double2* as = As[st];
-      const double2* bs = Bs[st];
-#pragma unroll
-      for (int ks = 0; ks < BK / 4; ++ks) {
-        double ar[4], ai[4], an[4], br[4], bi[4];
-#pragma unroll
-        for (int mt = 0; mt < 4; ++mt) {
-          const double2 v = as[sidx<A_K>(wm * 32 + mt * 8 + fr, ks * 4 + fk)];
-          ar[mt] = v.x;
-          ai[mt] = sa * v.y;
-          an[mt] = -ai[mt];
-        }
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-          const double2 v = bs[sidx<B_K>(wn * 32 + nt * 8 + fr, ks * 4 + fk)];
-          br[nt] = v.x;
-          bi[nt] = sb * v.y;
-        }
-#pragma unroll
-        // four passes over the 16 accumulator tiles: consecutive DMMAs never share an
-        // accumulator, so each waits on a result issued 16 instructions earlier
-        for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-          for (int nt = 0; nt < 4; ++nt) dmma(cr[mt][nt][0], cr[mt][nt][1], ar[mt], br[nt]);
-#pragma unroll
-        for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-          for (int nt = 0; nt < 4; ++nt) dmma(ci[mt][nt][0], ci[mt][nt][1], ar[mt], bi[nt]);
-#pragma unroll
-        for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-          for (int nt = 0; nt < 4; ++nt) dmma(cr[mt][nt][0], cr[mt][nt][1], an[mt], bi[nt]);
-#pragma unroll
-        for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-          for (int nt = 0; nt < 4; ++nt) dmma(ci[mt][nt][0], ci[mt][nt][1], ai[mt], br[nt]);
-      }
-      st = (st + 1 == STAGES) ? 0 : st + 1;
-      if (++cstep == per_tile) {
-        epilogue((tm0 + (span_m ? ctile : 0)) * BM, (tn0 + (span_m ? 0 : ctile)) * BN);
-        zero_acc();
-        cstep = 0;
-        ++ctile;
-      }
-    }
-    cp_wait<0>();
-  } else {
-    // one tile: prologue of STAGES-1 stages, then refill one stage per step
+  {
+    // prologue of STAGES-1 stages, then refill one stage per step
 #pragma unroll
     for (int s = 0; s < STAGES - 1; ++s) {
       if (t_begin + s < t_end) issue(t_begin + s, s);
@@ -314,6 +226,266 @@ __global__ void __launch_bounds__(NT, 2)
   }
 }
 
+// Eight-warp variant: the same 64 x 64 tile and 3-stage ring, 8 warps in a 2 x 4 layout with
+// 32 x 16 warp tiles (half the accumulators per thread, so two CTAs of 256 threads stay
+// resident at 128 registers).  It wins where the reduction is short (K = nao, runs of tiles per
+// CTA), the four-warp kernel where it is long.  G3 selects the three-product complex form.
+// The reduction position advances by counters (no division per step), and k quarters that
+// lie wholly past K are skipped.
+constexpr int NT8 = 256;
+constexpr int WARPS_M8 = 2;
+constexpr int WM8 = 32, WN8 = 16;
+constexpr int FM8 = WM8 / 8, FN8 = WN8 / 8;
+constexpr int SPT8 = TILE / NT8;
+static_assert(SPT8 * NT8 == TILE, "whole staging assignments");
+
+// index map with 32-bit division (indices of one operand are below 2^31)
+__device__ __forceinline__ long imap(const IdxMap& f, int i) {
+  return f.split > 0 ? (long)(i / f.split) * f.hi + (long)(i % f.split) * f.lo : (long)i * f.lo;
+}
+
+template <bool A_K, bool B_K, bool SPAN, bool G3>
+__global__ void __launch_bounds__(NT8, 2)
+    zgemm8_kernel(ZgemmDesc d, int tiles_m, int tiles_n, int span, int span_m) {
+  if (!SPAN) span = 1;
+  __shared__ __align__(16) double2 As[STAGES][TILE];
+  __shared__ __align__(16) double2 Bs[STAGES][TILE];
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int wm = warp % WARPS_M8, wn = warp / WARPS_M8;
+
+  const int groups_m = span_m ? (tiles_m + span - 1) / span : tiles_m;
+  const int groups_n = span_m ? tiles_n : (tiles_n + span - 1) / span;
+  const long bid = blockIdx.x;
+  const int ngroup = groups_m * groups_n;
+  const int group = (int)(bid % ngroup);
+  const long rest = bid / ngroup;
+  const int split = (int)(rest % d.splits);
+  const long batch = rest / d.splits;
+  const int b0 = (int)(batch % d.nb0);
+  const int b1 = (int)((batch / d.nb0) % d.nb1);
+  const int b2 = (int)(batch / ((long)d.nb0 * d.nb1));
+  const int gm = group % groups_m, gn = group / groups_m;
+  const int tm0 = span_m ? gm * span : gm, tn0 = span_m ? gn : gn * span;
+  const int ntiles = !SPAN ? 1 : span_m ? min(span, tiles_m - tm0) : min(span, tiles_n - tn0);
+
+  const double2* Ab = d.A + b0 * d.a_b0 + b1 * d.a_b1 + b2 * d.a_b2;
+  const double2* Bb = d.B + b0 * d.b_b0 + b1 * d.b_b1 + b2 * d.b_b2;
+
+  // staging: BM * BK elements per operand stage, SPT8 per thread
+  //   KMAJ : k = tid % BK, rows tid / BK + (NT8 / BK) i
+  //   !KMAJ: row = tid % BM, k = tid / BM + (NT8 / BM) i
+  long a_off[SPT8], b_off[SPT8];
+  bool a_ok[SPT8], b_ok[SPT8];
+  auto set_a = [&](int m0) {
+#pragma unroll
+    for (int i = 0; i < SPT8; ++i) {
+      const int m = m0 + (A_K ? tid / BK + (NT8 / BK) * i : tid % BM);
+      a_ok[i] = m < d.M;
+      a_off[i] = a_ok[i] ? imap(d.a_m, m) : 0;
+    }
+  };
+  auto set_b = [&](int n0) {
+#pragma unroll
+    for (int i = 0; i < SPT8; ++i) {
+      const int n = n0 + (B_K ? tid / BK + (NT8 / BK) * i : tid % BM);
+      b_ok[i] = n < d.N;
+      b_off[i] = b_ok[i] ? imap(d.b_n, n) : 0;
+    }
+  };
+  set_a(tm0 * BM);
+  set_b(tn0 * BN);
+
+  const int ktiles = (d.K + BK - 1) / BK;
+  const long total = (long)d.KB * ktiles;
+  const long t_begin = total * split / d.splits;
+  const long t_end = total * (split + 1) / d.splits;
+  const long per_tile = t_end - t_begin;
+  const int kb_begin = (int)(t_begin / ktiles), kt_begin = (int)(t_begin % ktiles);
+
+  // issue stream position: tile itile, reduction block ikb, k tile ikt (no divisions per step)
+  int itile = 0, ikb = kb_begin, ikt = kt_begin;
+  long icount = 0;
+  auto issue_next = [&](int st) {
+    if (itile >= ntiles) return;
+    const int k0 = ikt * BK;
+    const double2* Ak = Ab + ikb * d.a_kb;
+    const double2* Bk = Bb + ikb * d.b_kb;
+#pragma unroll
+    for (int i = 0; i < SPT8; ++i) {
+      const int r = A_K ? tid / BK + (NT8 / BK) * i : tid % BM;
+      const int kk = A_K ? tid % BK : tid / BM + (NT8 / BM) * i;
+      const int k = k0 + kk;
+      const bool v = a_ok[i] && k < d.K;
+      cp_async16(&As[st][sidx<A_K>(r, kk)], v ? (const void*)(Ak + a_off[i] + k * d.a_k) : (const void*)Ab, v);
+    }
+#pragma unroll
+    for (int i = 0; i < SPT8; ++i) {
+      const int r = B_K ? tid / BK + (NT8 / BK) * i : tid % BM;
+      const int kk = B_K ? tid % BK : tid / BM + (NT8 / BM) * i;
+      const int k = k0 + kk;
+      const bool v = b_ok[i] && k < d.K;
+      cp_async16(&Bs[st][sidx<B_K>(r, kk)], v ? (const void*)(Bk + b_off[i] + k * d.b_k) : (const void*)Bb, v);
+    }
+    if (++ikt == ktiles) {
+      ikt = 0;
+      ++ikb;
+    }
+    if (++icount == per_tile) {
+      icount = 0;
+      ikb = kb_begin;
+      ikt = kt_begin;
+      if (++itile < ntiles) {
+        if (span_m) set_a((tm0 + itile) * BM);
+        else set_b((tn0 + itile) * BN);
+      }
+    }
+  };
+
+  // accumulators: c0/c1 = re/im (four products) or c0/c1/c2 = rr, ii, (r+i)(r+i) (three)
+  double c0[FM8][FN8][2], c1[FM8][FN8][2], c2[FM8][FN8][2];
+  auto zero_acc = [&]() {
+#pragma unroll
+    for (int a = 0; a < FM8; ++a)
+#pragma unroll
+      for (int b = 0; b < FN8; ++b)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          c0[a][b][j] = 0.0;
+          c1[a][b][j] = 0.0;
+          if (G3) c2[a][b][j] = 0.0;
+        }
+  };
+  zero_acc();
+
+  const double sa = d.conjA ? -1.0 : 1.0;
+  const double sb = d.conjB ? -1.0 : 1.0;
+  const int fr = lane >> 2, fk = lane & 3;
+
+  auto epilogue = [&](int m0, int n0) {
+    const long batch_count = (long)d.nb0 * d.nb1 * d.nb2;
+    const double2* cbase = d.C + b0 * d.c_b0 + b1 * d.c_b1 + b2 * d.c_b2;
+    const bool use_beta = d.beta.x != 0.0 || d.beta.y != 0.0;
+#pragma unroll
+    for (int mt = 0; mt < FM8; ++mt) {
+      const int m = m0 + wm * WM8 + mt * 8 + fr;
+      if (m >= d.M) continue;
+      const long cm = imap(d.c_m, m);
+#pragma unroll
+      for (int nt = 0; nt < FN8; ++nt) {
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int n = n0 + wn * WN8 + nt * 8 + 2 * fk + j;
+          if (n >= d.N) continue;
+          const double2 acc = G3 ? make_double2(c0[mt][nt][j] - c1[mt][nt][j],
+                                                c2[mt][nt][j] - c0[mt][nt][j] - c1[mt][nt][j])
+                                 : make_double2(c0[mt][nt][j], c1[mt][nt][j]);
+          if (d.splits > 1) {
+            d.work[((split * batch_count + batch) * d.M + m) * (long)d.N + n] = acc;
+          } else {
+            double2* c = const_cast<double2*>(cbase) + cm + imap(d.c_n, n);
+            double2 v = cmul(d.alpha, acc);
+            if (use_beta) v = cadd(v, cmul(d.beta, *c));
+            *c = v;
+          }
+        }
+      }
+    }
+  };
+
+  auto substep = [&](const double2* as, const double2* bs, int ks) {
+    double ar[FM8], ai[FM8], ax[FM8], br[FN8], bi[FN8], bx[FN8];
+#pragma unroll
+    for (int mt = 0; mt < FM8; ++mt) {
+      const double2 v = as[sidx<A_K>(wm * WM8 + mt * 8 + fr, ks * 4 + fk)];
+      ar[mt] = v.x;
+      ai[mt] = sa * v.y;
+      ax[mt] = G3 ? ar[mt] + ai[mt] : -ai[mt];
+    }
+#pragma unroll
+    for (int nt = 0; nt < FN8; ++nt) {
+      const double2 v = bs[sidx<B_K>(wn * WN8 + nt * 8 + fr, ks * 4 + fk)];
+      br[nt] = v.x;
+      bi[nt] = sb * v.y;
+      bx[nt] = br[nt] + bi[nt];
+    }
+    if constexpr (G3) {
+#pragma unroll
+      for (int mt = 0; mt < FM8; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < FN8; ++nt) dmma(c0[mt][nt][0], c0[mt][nt][1], ar[mt], br[nt]);
+#pragma unroll
+      for (int mt = 0; mt < FM8; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < FN8; ++nt) dmma(c1[mt][nt][0], c1[mt][nt][1], ai[mt], bi[nt]);
+#pragma unroll
+      for (int mt = 0; mt < FM8; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < FN8; ++nt) dmma(c2[mt][nt][0], c2[mt][nt][1], ax[mt], bx[nt]);
+    } else {
+#pragma unroll
+      for (int mt = 0; mt < FM8; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < FN8; ++nt) dmma(c0[mt][nt][0], c0[mt][nt][1], ar[mt], br[nt]);
+#pragma unroll
+      for (int mt = 0; mt < FM8; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < FN8; ++nt) dmma(c1[mt][nt][0], c1[mt][nt][1], ar[mt], bi[nt]);
+#pragma unroll
+      for (int mt = 0; mt < FM8; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < FN8; ++nt) dmma(c0[mt][nt][0], c0[mt][nt][1], ax[mt], bi[nt]);
+#pragma unroll
+      for (int mt = 0; mt < FM8; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < FN8; ++nt) dmma(c1[mt][nt][0], c1[mt][nt][1], ai[mt], br[nt]);
+    }
+  };
+
+  // prologue: STAGES-1 stages in flight (with SPAN possibly reaching into the next tiles)
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    issue_next(s);
+    cp_commit();
+  }
+  int st = 0;
+  int ctile = 0, ckt = kt_begin;
+  long cstep = 0;
+  const long steps = (long)ntiles * per_tile;
+  for (long s = 0; s < steps; ++s) {
+    cp_wait<STAGES - 2>();
+    __syncthreads();
+    {
+      int sn = st + STAGES - 1;
+      if (sn >= STAGES) sn -= STAGES;
+      issue_next(sn);
+      cp_commit();
+    }
+    // k quarters wholly past K (zero-filled) are skipped
+    {
+      const int krem = d.K - ckt * BK;
+#pragma unroll
+      for (int ks = 0; ks < BK / 4; ++ks)
+        if (ks == 0 || krem > 4 * ks) substep(As[st], Bs[st], ks);
+    }
+    st = (st + 1 == STAGES) ? 0 : st + 1;
+    if (++ckt == ktiles) ckt = 0;
+    if constexpr (SPAN) {
+      if (++cstep == per_tile) {
+        epilogue((tm0 + (span_m ? ctile : 0)) * BM, (tn0 + (span_m ? 0 : ctile)) * BN);
+        zero_acc();
+        cstep = 0;
+        ckt = kt_begin;
+        ++ctile;
+      }
+    }
+  }
+  cp_wait<0>();
+  if constexpr (!SPAN) epilogue(tm0 * BM, tn0 * BN);
+}
+
 __global__ void zgemm_reduce(ZgemmDesc d) {
   const long batch_count = (long)d.nb0 * d.nb1 * d.nb2;
   const long mn = (long)d.M * d.N;
@@ -337,12 +509,28 @@ __global__ void zgemm_reduce(ZgemmDesc d) {
 }
 
 template <bool A_K, bool B_K>
-void launch(const ZgemmDesc& d, int tiles_m, int tiles_n, int span, int span_m, long blocks, cudaStream_t stream) {
-  if (span > 1)
-    zgemm_kernel<A_K, B_K, true><<<(unsigned)blocks, NT, 0, stream>>>(d, tiles_m, tiles_n, span, span_m);
-  else
-    zgemm_kernel<A_K, B_K, false><<<(unsigned)blocks, NT, 0, stream>>>(d, tiles_m, tiles_n, 1, 0);
+void launch(const ZgemmDesc& d, int tiles_m, int tiles_n, long blocks, cudaStream_t stream) {
+  zgemm_kernel<A_K, B_K><<<(unsigned)blocks, NT, 0, stream>>>(d, tiles_m, tiles_n);
   GG_CHECK_LAUNCH();
+}
+
+template <bool A_K, bool B_K, bool G3>
+void launch8(const ZgemmDesc& d, int tiles_m, int tiles_n, int span, int span_m, long blocks, cudaStream_t stream) {
+  if (span > 1)
+    zgemm8_kernel<A_K, B_K, true, G3><<<(unsigned)blocks, NT8, 0, stream>>>(d, tiles_m, tiles_n, span, span_m);
+  else
+    zgemm8_kernel<A_K, B_K, false, G3><<<(unsigned)blocks, NT8, 0, stream>>>(d, tiles_m, tiles_n, 1, 0);
+  GG_CHECK_LAUNCH();
+}
+
+template <bool G3>
+void launch8_layout(const ZgemmDesc& d, int tiles_m, int tiles_n, int span, int span_m, long blocks,
+                    cudaStream_t stream) {
+  const bool ak = (d.a_k == 1), bk = (d.b_k == 1);
+  if (ak && bk) launch8<true, true, G3>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  else if (ak) launch8<true, false, G3>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  else if (bk) launch8<false, true, G3>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  else launch8<false, false, G3>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
 }
 
 int sm_count() {
@@ -403,11 +591,16 @@ int zgemm(const ZgemmDesc& d0, cudaStream_t stream) {
                              : (long)tiles_m * ((tiles_n + span - 1) / span) * batch;
   const long blocks = groups * splits;
   if (blocks > 0x7fffffffL) throw Error(GG_ERR_ARG, "zgemm: grid too large");
+  // kernel choice (both 64 x 64 tiles, same grid): the three-product form always runs on the
+  // eight-warp kernel; the four-product form runs there for runs of tiles (short reductions)
+  // and on the four-warp kernel otherwise
   const bool ak = (d.a_k == 1), bk = (d.b_k == 1);
-  if (ak && bk) launch<true, true>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
-  else if (ak) launch<true, false>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
-  else if (bk) launch<false, true>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
-  else launch<false, false>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  if (d.gauss) launch8_layout<true>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  else if (span > 1) launch8_layout<false>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  else if (ak && bk) launch<true, true>(d, tiles_m, tiles_n, blocks, stream);
+  else if (ak) launch<true, false>(d, tiles_m, tiles_n, blocks, stream);
+  else if (bk) launch<false, true>(d, tiles_m, tiles_n, blocks, stream);
+  else launch<false, false>(d, tiles_m, tiles_n, blocks, stream);
   int launches = 1;
   if (splits > 1) {
     const long total = (long)d.M * d.N * batch;

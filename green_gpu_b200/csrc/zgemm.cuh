@@ -43,6 +43,11 @@ struct ZgemmDesc {
   double2 alpha = {1.0, 0.0};
   double2 beta = {0.0, 0.0};
   int conjA = 0, conjB = 0;
+  // 1: three real products per complex product, re = ar br - ai bi and
+  // im = (ar + ai)(br + bi) - ar br - ai bi (normwise error still O(u K |A||B|), about
+  // 1e-16 relative, but not componentwise).  Used only inside the split-precision build, whose
+  // error budget is six orders larger; the FP64 path keeps the four-product form.
+  int gauss = 0;
   int splits = 1;            // split-K factor (deterministic: partials + ordered reduction)
   double2* work = nullptr;   // [splits][batch][M][N] when splits > 1
   long work_elems = 0;       // capacity of `work` in complex elements
