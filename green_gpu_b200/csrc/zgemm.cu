@@ -226,16 +226,15 @@ __global__ void __launch_bounds__(NT, 2)
   }
 }
 
-// Eight-warp variant: the same 64 x 64 tile and 3-stage ring, 8 warps in a 2 x 4 layout with
-// 32 x 16 warp tiles (half the accumulators per thread, so two CTAs of 256 threads stay
-// resident at 128 registers).  It wins where the reduction is short (K = nao, runs of tiles per
-// CTA), the four-warp kernel where it is long.  G3 selects the three-product complex form.
-// The reduction position advances by counters (no division per step), and k quarters that
-// lie wholly past K are skipped.
+// Eight-warp variant: the same 64 x 64 tile and 3-stage ring, 8 warps of 16 x 32 (4 x 2
+// layout; half the accumulators per thread, so two CTAs of 256 threads stay resident at 128
+// registers).  It wins where the reduction is short (K = nao, runs of tiles per CTA), the
+// four-warp kernel where it is long.  G3 selects the three-product complex form.  NARROW (N <=
+// 56, a single column tile): 8 warps of 8 x 56, so the MMAs cover columns 0..55 only (N = nao
+// = 52 fills 93 % of them instead of 81 % of 64) and every warp has the same work.  The
+// reduction position advances by counters (no division per step), and k quarters that lie
+// wholly past K are skipped.
 constexpr int NT8 = 256;
-constexpr int WARPS_M8 = 2;
-constexpr int WM8 = 32, WN8 = 16;
-constexpr int FM8 = WM8 / 8, FN8 = WN8 / 8;
 constexpr int SPT8 = TILE / NT8;
 static_assert(SPT8 * NT8 == TILE, "whole staging assignments");
 
@@ -244,7 +243,7 @@ __device__ __forceinline__ long imap(const IdxMap& f, int i) {
   return f.split > 0 ? (long)(i / f.split) * f.hi + (long)(i % f.split) * f.lo : (long)i * f.lo;
 }
 
-template <bool A_K, bool B_K, bool SPAN, bool G3>
+template <bool A_K, bool B_K, bool SPAN, bool G3, bool NARROW>
 __global__ void __launch_bounds__(NT8, 2)
     zgemm8_kernel(ZgemmDesc d, int tiles_m, int tiles_n, int span, int span_m) {
   if (!SPAN) span = 1;
@@ -254,6 +253,9 @@ __global__ void __launch_bounds__(NT8, 2)
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
+  constexpr int WARPS_M8 = NARROW ? 8 : 4;
+  constexpr int WM8 = NARROW ? 8 : 16, WN8 = NARROW ? 56 : 32;
+  constexpr int FM8 = WM8 / 8, FN8 = WN8 / 8;
   const int wm = warp % WARPS_M8, wn = warp / WARPS_M8;
 
   const int groups_m = span_m ? (tiles_m + span - 1) / span : tiles_m;
@@ -514,23 +516,30 @@ void launch(const ZgemmDesc& d, int tiles_m, int tiles_n, long blocks, cudaStrea
   GG_CHECK_LAUNCH();
 }
 
-template <bool A_K, bool B_K, bool G3>
+template <bool A_K, bool B_K, bool G3, bool NARROW>
 void launch8(const ZgemmDesc& d, int tiles_m, int tiles_n, int span, int span_m, long blocks, cudaStream_t stream) {
   if (span > 1)
-    zgemm8_kernel<A_K, B_K, true, G3><<<(unsigned)blocks, NT8, 0, stream>>>(d, tiles_m, tiles_n, span, span_m);
+    zgemm8_kernel<A_K, B_K, true, G3, NARROW><<<(unsigned)blocks, NT8, 0, stream>>>(d, tiles_m, tiles_n, span, span_m);
   else
-    zgemm8_kernel<A_K, B_K, false, G3><<<(unsigned)blocks, NT8, 0, stream>>>(d, tiles_m, tiles_n, 1, 0);
+    zgemm8_kernel<A_K, B_K, false, G3, NARROW><<<(unsigned)blocks, NT8, 0, stream>>>(d, tiles_m, tiles_n, 1, 0);
   GG_CHECK_LAUNCH();
 }
 
-template <bool G3>
+template <bool G3, bool NARROW>
 void launch8_layout(const ZgemmDesc& d, int tiles_m, int tiles_n, int span, int span_m, long blocks,
                     cudaStream_t stream) {
   const bool ak = (d.a_k == 1), bk = (d.b_k == 1);
-  if (ak && bk) launch8<true, true, G3>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
-  else if (ak) launch8<true, false, G3>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
-  else if (bk) launch8<false, true, G3>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
-  else launch8<false, false, G3>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  if (ak && bk) launch8<true, true, G3, NARROW>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  else if (ak) launch8<true, false, G3, NARROW>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  else if (bk) launch8<false, true, G3, NARROW>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  else launch8<false, false, G3, NARROW>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+}
+
+template <bool G3>
+void launch8_any(const ZgemmDesc& d, int tiles_m, int tiles_n, int span, int span_m, long blocks,
+                 cudaStream_t stream) {
+  if (d.N <= 56) launch8_layout<G3, true>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  else launch8_layout<G3, false>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
 }
 
 int sm_count() {
@@ -595,8 +604,8 @@ int zgemm(const ZgemmDesc& d0, cudaStream_t stream) {
   // eight-warp kernel; the four-product form runs there for runs of tiles (short reductions)
   // and on the four-warp kernel otherwise
   const bool ak = (d.a_k == 1), bk = (d.b_k == 1);
-  if (d.gauss) launch8_layout<true>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
-  else if (span > 1) launch8_layout<false>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  if (d.gauss) launch8_any<true>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
+  else if (span > 1) launch8_any<false>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
   else if (ak && bk) launch<true, true>(d, tiles_m, tiles_n, blocks, stream);
   else if (ak) launch<true, false>(d, tiles_m, tiles_n, blocks, stream);
   else if (bk) launch<false, true>(d, tiles_m, tiles_n, blocks, stream);
