@@ -329,6 +329,19 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
     }
   };
 
+  // the O(nao^3 NQ) operand builds of P0 (G V and V^+ G) also run on the INT8 engine in split
+  // precision: their large operand V is sliced once per launch for the whole tau block and
+  // the G operand is small, so slicing costs little next to the FP64 GEMM it replaces
+  auto gemm_build = [&](ZgemmDesc d) {
+    if (split) {
+      d.work = gw_work;
+      d.work_elems = (long)c->gemm_work.n;
+      c->launches += split_zgemm(split, d, c->slices, st);
+    } else {
+      gemm(d);
+    }
+  };
+
   // pair tables: P0 pairs (k, k+q) for every irreducible q, Sigma pairs (k_ibz, k_ibz - q');
   // G1 block indices: block (k1 * ns + sp) of Gf, for every (iq, sp, k).  Built once per
   // symmetry / k-pair / spin setting (the uploads synchronise, so never while capturing).
@@ -410,7 +423,7 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
               d.c_n.split = n; d.c_n.hi = nn; d.c_n.lo = 1;
               d.nb0 = kn;
               d.a_b0 = (long)ns * T * nn; d.b_b0 = Nnn; d.c_b0 = (long)tn * Nnn;
-              gemm(d);
+              gemm_build(d);
             }
             // B-build: SB[kk][tt][Q][a][b] = sum_l conj(V[kk][Q][a][l]) G^{k+q}(tau_t)[b][l],
             // tau folded into the columns, n = (tt, b)
@@ -422,7 +435,7 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
               d.C = SB; d.c_m.lo = n; d.c_n.split = n; d.c_n.hi = Nnn; d.c_n.lo = 1;
               d.nb0 = kn;
               d.a_b0 = Nnn; d.b_b0 = (long)T2 * nn; d.c_b0 = (long)tn * Nnn;
-              gemm(d);
+              gemm_build(d);
             }
             // P0[q][t] (+)= pref/nk sum_kk sum_x SA[kk][tt][Q'][x] SB[kk][tt][Q][x]
             {
