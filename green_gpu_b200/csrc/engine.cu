@@ -332,11 +332,21 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
   // the O(nao^3 NQ) operand builds of P0 (G V and V^+ G) also run on the INT8 engine in split
   // precision: their large operand V is sliced once per launch for the whole tau block and
   // the G operand is small, so slicing costs little next to the FP64 GEMM it replaces
+  // The INT8 engine's epilogue gives each lane one row of C, so its stores coalesce when C is
+  // contiguous along m; the build outputs are contiguous along n, so they are computed as
+  // C^T = B^T A^T (the same slices and int32 sums, so the same result).
   auto gemm_build = [&](ZgemmDesc d) {
     if (split) {
-      d.work = gw_work;
-      d.work_elems = (long)c->gemm_work.n;
-      c->launches += split_zgemm(split, d, c->slices, st);
+      ZgemmDesc t = d;
+      t.M = d.N; t.N = d.M;
+      t.A = d.B; t.a_m = d.b_n; t.a_k = d.b_k; t.a_kb = d.b_kb; t.conjA = d.conjB;
+      t.a_b0 = d.b_b0; t.a_b1 = d.b_b1; t.a_b2 = d.b_b2;
+      t.B = d.A; t.b_n = d.a_m; t.b_k = d.a_k; t.b_kb = d.a_kb; t.conjB = d.conjA;
+      t.b_b0 = d.a_b0; t.b_b1 = d.a_b1; t.b_b2 = d.a_b2;
+      t.c_m = d.c_n; t.c_n = d.c_m;
+      t.work = gw_work;
+      t.work_elems = (long)c->gemm_work.n;
+      c->launches += split_zgemm(split, t, c->slices, st);
     } else {
       gemm(d);
     }
