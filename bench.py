@@ -117,78 +117,117 @@ def make_inputs(cfg, device, seed=0):
     return s, V
 
 
-def oracle_cpu_baseline(cfg, budget_s=20.0):
-    """Time the FP64 oracle on a bounded sample of the workload and extrapolate to builds/s.
+def _blas_threads():
+    try:
+        from threadpoolctl import threadpool_info
+        n = [d.get("num_threads") for d in threadpool_info() if d.get("user_api") == "blas"]
+        if n and n[0]:
+            return int(n[0])
+    except Exception:
+        pass
+    return os.cpu_count()
 
-    Sample: P0 of one q over a few k, Sigma of a few (k, q') pairs, Dyson + IR of one q;
-    a build is nq*nk P0 pairs + nq (IR + Dyson) + ink*nq Sigma pairs.
+
+class CpuSample:
+    """The FP64 oracle on a bounded sample of one GW build of the configured system.
+
+    Set-up (once): a system with the configured nao / NQ / tau grid and a 2-pair k store (the
+    per-pair cost does not depend on the k mesh), the full-BZ G and one W~(tau).  One sample
+    times one P0 (q, k) pair, one q of IR transforms + Dyson (all nw_b frequencies) and one
+    Sigma (k, q') pair; a build is nk^2 P0 pairs + nq q steps + nk * nq Sigma pairs (full BZ,
+    identity symmetry), so the extrapolated build time is nk^2 (t_p0 + t_sigma) + nk t_q.
     """
-    import oracle.gw as ogw
-    from green_gpu_b200 import synth
-    s = synth.make_system(seed=1, **CONFIGS[cfg]) if cfg == "cfg1" else None
-    if s is None:
-        # cfg2-shaped sample with a 2-pair store (the per-pair cost does not depend on nk)
-        s = synth.make_system(mesh=(2, 1, 1), nao=CONFIGS[cfg]["nao"], NQ=CONFIGS[cfg]["NQ"], seed=1)
-    nts, nk = s.nts, s.nk
-    Gf = ogw.g_full(s)
-    tt = np.arange(nts // 2)
-    pref = -2.0
-    t0 = time.perf_counter()
-    n_p0 = 0
-    from oracle.symmetry import coulomb
-    while time.perf_counter() - t0 < budget_s * 0.4 or n_p0 == 0:
-        k = n_p0 % nk
-        k1 = int(s.k1_from_k2q[k * s.nq + 0])
-        V = coulomb(s, k, k1)
-        ogw.p0_pair(V, Gf[k1, 0, tt], Gf[k, 0, nts - 1 - tt], pref)
-        n_p0 += 1
-    t_p0 = (time.perf_counter() - t0) / n_p0
-    t0 = time.perf_counter()
-    P0 = np.zeros((nts, s.NQ, s.NQ), np.complex128)
-    for t in range(nts):
-        X = np.random.default_rng(t).standard_normal((s.NQ, s.NQ)) * 1e-3
-        P0[t] = -(X @ X.T)
-    Pw = ogw.transform_tw(P0, s.Tnt_BF)
-    Ww = ogw.dyson(Pw, "cholesky")
-    Wt = ogw.transform_wt(Ww, s.Ttn_FB)
-    t_q = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    n_sg = 0
-    while time.perf_counter() - t0 < budget_s * 0.4 or n_sg == 0:
-        k1 = int(s.k2_from_k1q[0 * s.nq + (n_sg % nk)])
-        V = coulomb(s, 0, k1)
-        ogw.sigma_pair(V, Gf[k1, 0], Wt)
-        n_sg += 1
-    t_sg = (time.perf_counter() - t0) / n_sg
-    NK = int(np.prod(CONFIGS[cfg]["mesh"]))
-    t_build = NK * NK * t_p0 + NK * t_q + NK * NK * t_sg
-    cores = os.cpu_count()
-    return {"value": 1.0 / t_build, "unit": "builds/s", "cores": cores, "kind": "port",
-            "sample": f"numpy FP64 oracle, {cfg}: {n_p0} P0 (q,k) pairs, 1 q of IR+Dyson, {n_sg} Sigma (k,q') "
-                      f"pairs timed; per-pair times x {NK}x{NK} pairs + {NK} q; OpenBLAS threads = all cores",
-            "seconds_per_build": t_build}
+
+    def __init__(self, cfg):
+        import oracle.gw as ogw
+        from green_gpu_b200 import synth
+        from oracle.symmetry import coulomb
+        self.ogw = ogw
+        c = CONFIGS[cfg]
+        self.cfg = cfg
+        self.NK = int(np.prod(c["mesh"]))
+        if cfg == "cfg1":
+            s = synth.make_system(seed=1, **c)
+        else:
+            s = synth.make_system(mesh=(2, 1, 1), nao=c["nao"], NQ=c["NQ"], seed=1)
+        self.s = s
+        self.Gf = ogw.g_full(s)
+        self.pairs = []
+        for k in range(s.nk):
+            k1 = int(s.k1_from_k2q[k * s.nq + 0])
+            self.pairs.append((k, k1, coulomb(s, k, k1)))
+        P0 = np.zeros((s.nts, s.NQ, s.NQ), np.complex128)
+        for t in range(s.nts):
+            X = np.random.default_rng(t).standard_normal((s.NQ, s.NQ)) * 1e-3
+            P0[t] = -(X @ X.T)
+        self.P0 = P0
+        self.Wt = ogw.transform_wt(ogw.dyson(ogw.transform_tw(P0, s.Tnt_BF)), s.Ttn_FB)
+        n, N, T = s.nao, s.NQ, s.nts
+        # reference FLOP model (8MNK + 12MN per complex GEMM, src/green/gpu/common_defs.h:121-125)
+        self.f_p0 = (T // 2) * (2 * (8.0 * n * N * n * n) + 8.0 * N * N * n * n)
+        self.f_sg = T * (2 * (8.0 * N * n * n * n) + 8.0 * N * N * n * n)
+        self.i = 0
+
+    def step(self):
+        s, ogw = self.s, self.ogw
+        nts = s.nts
+        tt = np.arange(nts // 2)
+        k, k1, V = self.pairs[self.i % len(self.pairs)]
+        self.i += 1
+        t0 = time.perf_counter()
+        ogw.p0_pair(V, self.Gf[k1, 0, tt], self.Gf[k, 0, nts - 1 - tt], -2.0)
+        t1 = time.perf_counter()
+        ogw.transform_wt(ogw.dyson(ogw.transform_tw(self.P0, s.Tnt_BF)), s.Ttn_FB)
+        t2 = time.perf_counter()
+        ogw.sigma_pair(V, self.Gf[k1, 0], self.Wt)
+        t3 = time.perf_counter()
+        t_p0, t_q, t_sg = t1 - t0, t2 - t1, t3 - t2
+        return {"t_p0": t_p0, "t_q": t_q, "t_sigma": t_sg,
+                "seconds_per_build": self.NK * self.NK * (t_p0 + t_sg) + self.NK * t_q,
+                "sample_s": t3 - t0}
+
+    def describe(self, steps):
+        tp = statistics.median([x["t_p0"] for x in steps])
+        ts = statistics.median([x["t_sigma"] for x in steps])
+        tq = statistics.median([x["t_q"] for x in steps])
+        return (f"numpy FP64 oracle (OpenBLAS, {_blas_threads()} threads), {self.cfg}: per sample 1 P0 (q,k) pair "
+                f"({tp:.2f} s, {self.f_p0 / tp / 1e9:.0f} GFLOP/s), 1 q of IR + Dyson over {self.s.nw_b} "
+                f"frequencies ({tq:.2f} s), 1 Sigma (k,q') pair ({ts:.2f} s, {self.f_sg / ts / 1e9:.0f} GFLOP/s); "
+                f"build = {self.NK}^2 x (P0 + Sigma pair) + {self.NK} q steps; {len(steps)} samples")
+
+
+def oracle_cpu_baseline(cfg, samples=3, sampler=None):
+    """Timed CPU baseline (rank 0, N = 1): a few samples of the oracle, extrapolated to builds/s."""
+    cs = sampler or CpuSample(cfg)
+    steps = [cs.step() for _ in range(samples)]
+    t_build = statistics.median([x["seconds_per_build"] for x in steps])
+    return {"value": 1.0 / t_build, "unit": "builds/s", "cores": _blas_threads(), "kind": "port",
+            "sample": cs.describe(steps), "seconds_per_build": t_build}
 
 
 def run_reference(args):
     """Reference arm: the reference's CPU path is the oracle port here (the reference itself
-    cannot be built: MPI, HDF5, Eigen and the green-* repositories are absent)."""
+    cannot be built: MPI, HDF5, Eigen and the green-* repositories are absent).  Each step is
+    one bounded sample of the build (one P0 pair, one q of IR + Dyson, one Sigma pair),
+    extrapolated to a whole build."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    steps = []
-    cb = None
-    for _ in range(args.warmup + args.steps):
-        cb = oracle_cpu_baseline(args.config, budget_s=4.0)
-        steps.append(cb["seconds_per_build"])
+    cs = CpuSample(args.config)
+    steps = [cs.step() for _ in range(args.warmup + args.steps)]
     timed = steps[args.warmup:]
-    v = len(timed) / sum(timed)
+    t_build = [x["seconds_per_build"] for x in timed]
+    v = len(t_build) / sum(t_build)
     line = {"metric": "GW Sigma builds/s", "value": v, "unit": "builds/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(timed) / len(timed),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(t_build) / len(t_build),
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-        "dtype": "c128" if args.precision == "fp64" else "c128 in/out, int8 slices on tensor cores",
-            "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"GW Sigma build, {args.config}", **{k: str(v_) for k, v_ in CONFIGS[args.config].items()}},
-            "cpu_baseline": {**{k: cb[k] for k in ("unit", "cores", "kind", "sample")}, "value": v},
+            "dtype": "c128", "data": "synthetic (seeded G from random Hermitian Fock, Gaussian V*exp(-0.1Q))",
+            "impl": "reference",
+            "config": {"workload": f"GW Sigma build {args.config}",
+                       "mesh": "x".join(map(str, CONFIGS[args.config]["mesh"])), "nao": CONFIGS[args.config]["nao"],
+                       "NQ": CONFIGS[args.config]["NQ"], "precision": "fp64"},
+            "cpu_baseline": {"value": v, "unit": "builds/s", "cores": _blas_threads(), "kind": "port",
+                             "sample": cs.describe(timed)},
             "e2e": {"value": v, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -205,6 +244,8 @@ def main():
     ap.add_argument("--slices", type=int, default=5)
     ap.add_argument("--solver", default="cholesky", choices=["cholesky", "lu"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="eager builds instead of graph replays")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 build of the same system")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -247,18 +288,18 @@ def main():
         if world > 1:
             dist.all_reduce(Sigma)
 
+    # graph mode: the first warm-up build runs eagerly and is captured; the later builds replay
+    # the captured graph (one launch per build).  No profiling events inside the timed region.
+    ctx.set_graph(not args.no_graph)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize(dev)
-    ctx.set_profiling(True)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     lat = []
-    launches = 0
-    kstats = {w: [0, 0.0, 0.0] for w in (0, 1, 2)}
     with ClockSampler(local) as clk:
         e0.record(stream)
         for _ in range(args.steps):
@@ -269,21 +310,27 @@ def main():
             b.record(stream)
             b.synchronize()
             lat.append(a.elapsed_time(b) * 1e-3)
-            launches += ctx.launch_count()
-            for w in (0, 1, 2):
-                st = ctx.kernel_stats(w)
-                kstats[w][0] += st["launches"]
-                kstats[w][1] += st["seconds"]
-                kstats[w][2] += st["flops"]
         e1.record(stream)
         torch.cuda.synchronize(dev)
-    ctx.set_profiling(False)
     elapsed = e0.elapsed_time(e1) * 1e-3
     if world > 1:
         t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed = float(t.item())
     value = args.steps / elapsed
+
+    # one profiled build after the timed region (eager, CUDA events around every launch of the
+    # dominant contractions): the per-kernel figures of the roofline and the launch count
+    ctx.set_profiling(True)
+    step()
+    torch.cuda.synchronize(dev)
+    ctx.set_profiling(False)
+    launches_per_build = ctx.launch_count()
+    phases = ctx.timings()
+    kstats = {w: [0, 0.0, 0.0] for w in (0, 1, 2)}
+    for w in (0, 1, 2):
+        st = ctx.kernel_stats(w)
+        kstats[w] = [st["launches"], st["seconds"], st["flops"]]
 
     # end to end through the host-buffer C ABI call (H2D of G from pinned memory, D2H of Sigma)
     e2e_vals = []
@@ -319,17 +366,20 @@ def main():
     dom = max((0, 1, 2), key=lambda w: kstats[w][1])
     n_l, sec, fl = kstats[dom]
     achieved = fl / sec / 1e12 if sec > 0 else 0.0
-    fp64_peak = float(os.environ.get("GG_FP64_PEAK_TFLOPS", "40.0"))
+    # the dominant kernels run inside a build of tens of seconds: sustained peaks
+    fp64_peak = float(os.environ.get("GG_FP64_PEAK_TFLOPS", "37.0"))
     kname = ("p0_contraction", "sigma_contraction", "sigma_final_contraction")[dom]
     if args.precision == "fp64":
-        peak, peak_note = fp64_peak, "nominal FP64 tensor (DMMA) peak of B200; no measured FP64 figure"
+        peak, peak_note = fp64_peak, ("FP64 tensor (DMMA) rate measured on this pool's B200 with a register-only "
+                                      "mma.sync f64 loop (37 TF/s; not part of MEASURED_PEAKS.json)")
         unit = "TFLOP/s"
         kname += " (FP64 DMMA zgemm)"
     else:
         # executed INT8 work: S(S+1)/2 slice pairs, each a real GEMM of 8MNK ops per complex GEMM
         pairs = args.slices * (args.slices + 1) // 2
         achieved *= pairs
-        peak, peak_note = 2.0 * pk["bf16_tflops"], f"2x {pk_src} bf16 burst (dense INT8 rate)"
+        peak, peak_note = (2.0 * pk["bf16_tflops_sustained"],
+                           f"2x {pk_src} bf16 sustained (dense INT8 rate; the kernel runs inside a long build)")
         unit = "TOP/s (int8)"
         kname += f" (slicing + tcgen05 INT8 GEMM, {args.slices} slices)"
     roof = {"bound": "tensor", "kernel": kname,
@@ -359,24 +409,44 @@ def main():
                    "parallelism": f"q-shard x{world}" if world > 1 else "1 GPU"},
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
         "model_tflops": flops_build * value / 1e12,
-        "phases_s": ctx.timings(),
+        "phases_s": phases,
         "roofline": roof,
-        "gpu_launches": launches,
+        "gpu_launches": launches_per_build * args.steps,
+        "timed_region": ("graph replays, no profiling events" if not args.no_graph else "eager builds, no profiling "
+                         "events") + "; phases_s and roofline from one profiled eager build after it",
         "clocks": clk.summary(),
         "e2e": {"value": (1.0 / statistics.mean(e2e_t)) if e2e_t else None, "unit": "builds/s",
                 "h2d_bytes_per_step": gbytes, "d2h_bytes_per_step": gbytes},
     }
-    if rank == 0 and args.precision == "split":
-        # accuracy of the split path against FP64 on the 2x2x2 k, nao 26, NQ 120 system
-        from green_gpu_b200 import synth as _synth
-        s1 = _synth.make_system(seed=7, **CONFIGS["cfg1"])
-        c1 = native.context_for(s1, device=local)
-        c1.set_split_slices(args.slices)
-        r64 = c1.gw_sigma(s1.G_tskij, solver=solver, precision=native.PREC_FP64)
-        rsp = c1.gw_sigma(s1.G_tskij, solver=solver, precision=native.PREC_SPLIT)
-        line["accuracy"] = {"sigma_max_rel_err_vs_fp64": float(np.abs(rsp - r64).max() / np.abs(r64).max()),
-                            "system": "cfg1 (2x2x2 k, nao 26, NQ 120)", "slices": args.slices}
-        c1.close()
+    if world == 1 and args.precision == "split" and not args.no_fp64:
+        # the same build in plain FP64 on the same inputs: its speed and the split path's error
+        # against it (Sigma and the HF exchange K of the benchmarked system)
+        ctx.set_graph(False)
+        Sigma64 = torch.empty_like(G)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ctx.gw_sigma_device(G.data_ptr(), Sigma64.data_ptr(), solver=solver, precision=native.PREC_FP64,
+                            stream=stream.cuda_stream)
+        b.record(stream)
+        b.synchronize()
+        t64 = a.elapsed_time(b) * 1e-3
+        sc = torch.view_as_complex(Sigma.view(-1, 2))
+        s64 = torch.view_as_complex(Sigma64.view(-1, 2))
+        err = float((sc - s64).abs().max() / s64.abs().max())
+        ctx.set_hf_precision(native.PREC_FP64)
+        K64 = ctx.hf_exchange(s.dm)
+        ctx.set_hf_precision(native.PREC_SPLIT)
+        Ksp = ctx.hf_exchange(s.dm)
+        ctx.set_hf_precision(native.PREC_FP64)
+        line["fp64"] = {"value": 1.0 / t64, "unit": "builds/s", "ms_per_step": 1e3 * t64, "steps": 1,
+                        "note": "one eager FP64 build of the same system on the same inputs, CUDA events",
+                        "split_speedup": value * t64}
+        line["accuracy"] = {"sigma_max_rel_err_vs_fp64": err,
+                            "k_max_rel_err_vs_fp64": float(np.abs(Ksp - K64).max() / np.abs(K64).max()),
+                            "system": f"{args.config} (the benchmarked system)", "slices": args.slices,
+                            "tolerance": 1e-8}
+        del Sigma64
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = oracle_cpu_baseline(args.config)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}

@@ -53,6 +53,20 @@ void check_shape(const gg_shape& s) {
 
 void gg::set_thread_error(const std::string& msg) { g_create_error = msg; }
 
+template <typename F>
+static int guarded_global(F&& f) {
+  try {
+    f();
+    return GG_OK;
+  } catch (const Error& e) {
+    gg::set_thread_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    gg::set_thread_error(e.what());
+    return GG_ERR_INTERNAL;
+  }
+}
+
 extern "C" {
 
 const char* gg_version(void) { return "green-b200 0.1 (sm_100a; FP64 DMMA engine)"; }
@@ -231,6 +245,15 @@ int gg_set_q_shard(gg_context* c, int rank, int size) {
   });
 }
 
+int gg_q_shard_points(int32_t inq, int rank, int size, int32_t* q_out, int32_t capacity, int32_t* count) {
+  return guarded_global([&] {
+    if (!count || (capacity > 0 && !q_out) || capacity < 0) throw Error(GG_ERR_ARG, "q shard points: bad buffers");
+    const std::vector<int> q = shard_q_points(inq, rank, size);
+    *count = (int32_t)q.size();
+    for (size_t i = 0; i < q.size() && (int32_t)i < capacity; ++i) q_out[i] = q[i];
+  });
+}
+
 int gg_set_split_slices(gg_context* c, int slices) {
   return guarded(c, [&] {
     c->invalidate();  // tables and captured graph depend on this setting
@@ -289,6 +312,16 @@ static cudaGraphExec_t capture_graph(const std::vector<gg_context*>& ctxs, cudaS
   return ex;
 }
 
+std::vector<const void*> gg_context::buffer_signature() const {
+  std::vector<const void*> v = {V,       V_owned.p, Uk.p,      Uq.p,    k_f2r_d.p,   k_tr_d.p,   Ttn.p,
+                                Tnt_fold.p, x2c_in.p, x2c_out.p, G_in.p, Sigma_out.p, Gf.p,       Gtmp.p,
+                                Vbuf.p,  G1buf.p,   scratchA.p, scratchB.p, P0buf.p, Pw.p,     Afac.p,
+                                Wt.p,    Wrot.p,    gemm_work.p, hf_D.p,  hf_F.p,      hf_c.p,     hf_J.p,
+                                info.p,  piv.p,     idx_i.p,   pos_d.p,  op_d.p,      gw_err.p,   gw_tables.get()};
+  split_buffers(split, v);
+  return v;
+}
+
 extern "C" {
 
 // after a replay: the Dyson status recorded on the device and the split engine's flag
@@ -305,7 +338,7 @@ static void gw_device(gg_context* c, const double2* G, double2* Sigma, int solve
     return;
   }
   if (c->graph_exec && c->graph_G == G && c->graph_S == Sigma && c->graph_solver == solver &&
-      c->graph_prec == precision && c->graph_stream == st) {
+      c->graph_prec == precision && c->graph_stream == st && c->graph_sig == c->buffer_signature()) {
     GG_CUDA(cudaGraphLaunch(c->graph_exec, st));
     GG_CUDA(cudaStreamSynchronize(st));
     graph_check(c, solver);
@@ -316,6 +349,7 @@ static void gw_device(gg_context* c, const double2* G, double2* Sigma, int solve
   c->drop_graph();
   gw_sequence(c, G, Sigma, solver, precision, st);
   c->graph_exec = capture_graph({c}, st, [&] { gw_sequence(c, G, Sigma, solver, precision, st); });
+  c->graph_sig = c->buffer_signature();
   c->graph_G = G;
   c->graph_S = Sigma;
   c->graph_solver = solver;
@@ -354,6 +388,7 @@ struct gg_batch {
   cudaEvent_t fork = nullptr;
   std::vector<cudaEvent_t> join;
   cudaGraphExec_t exec = nullptr;
+  std::vector<std::vector<const void*>> sig;  // each member's buffer addresses at capture
   ~gg_batch() {
     if (exec) cudaGraphExecDestroy(exec);
     for (auto e : join) cudaEventDestroy(e);
@@ -363,20 +398,6 @@ struct gg_batch {
 };
 
 }  // extern "C"
-
-template <typename F>
-static int guarded_global(F&& f) {
-  try {
-    f();
-    return GG_OK;
-  } catch (const Error& e) {
-    gg::set_thread_error(e.what());
-    return e.code;
-  } catch (const std::exception& e) {
-    gg::set_thread_error(e.what());
-    return GG_ERR_INTERNAL;
-  }
-}
 
 extern "C" {
 
@@ -423,6 +444,7 @@ int gg_batch_create(gg_context* const* ctxs, int n, const void* const* G, void* 
         GG_CUDA(cudaStreamWaitEvent(b->master, b->join[i], 0));
       }
     });
+    for (auto* c : b->ctx) b->sig.push_back(c->buffer_signature());
     *out = b.release();
   });
 }
@@ -431,6 +453,13 @@ int gg_batch_run(gg_batch* b, void* stream) {
   return guarded_global([&] {
     if (!b) throw Error(GG_ERR_ARG, "batch: NULL");
     GG_CUDA(cudaSetDevice(b->ctx[0]->device));
+    // a member context whose buffers moved since the capture (another entry point grew them,
+    // or a setter replaced its tables) would make the graph touch freed memory: refuse
+    for (size_t i = 0; i < b->ctx.size(); ++i)
+      if (b->ctx[i]->buffer_signature() != b->sig[i])
+        throw Error(GG_ERR_STATE, "batch system " + std::to_string(i) +
+                                      ": its context was changed or its buffers reallocated after the batch was "
+                                      "captured; destroy the batch and create it again");
     cudaStream_t st = stream ? (cudaStream_t)stream : b->master;
     GG_CUDA(cudaGraphLaunch(b->exec, st));
     GG_CUDA(cudaStreamSynchronize(st));

@@ -43,4 +43,10 @@ inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
 // message returned by gg_last_error(NULL) on this thread (capi.cu)
 void set_thread_error(const std::string& msg);
 
+// number of SMs of the current device, looked up once per device (zgemm.cu)
+int device_sm_count();
+// index of the current device, checked against the per-device caches' capacity (zgemm.cu)
+constexpr int kMaxDevices = 64;
+int current_device();
+
 }  // namespace gg

@@ -80,7 +80,7 @@ struct gg_context {
   bool has_ir = false;
   gg::DevBuf<double2> Ttn, Tnt_fold;
 
-  int slices = 4;
+  int slices = GG_DEFAULT_SPLIT_SLICES;
   int hf_precision = GG_PREC_FP64;
   // two-component (X2C) mode: inputs and outputs are spinor matrices of order 2 nao; GW runs
   // on the four spin blocks as pseudo-spins (aa, bb, ab, ba), HF on three (aa, bb, ab)
@@ -122,6 +122,9 @@ struct gg_context {
   void* graph_S = nullptr;
   int graph_solver = -1, graph_prec = -1;
   cudaStream_t graph_stream = nullptr;
+  // device addresses of every work buffer when the graph was captured: an entry point that
+  // grows a shared buffer (HF, unfold, zgemm) reallocates it, and the graph is then rebuilt
+  std::vector<const void*> graph_sig;
   gg::DevBuf<int> gw_err;  // [0] failed, [1] system index (q position x nw_b + Omega), [2] info
   int plan_qc = 0, plan_kc = 0, plan_tb = 0;  // plan of the eager build, reused by the capture
 
@@ -130,7 +133,10 @@ struct gg_context {
     graph_exec = nullptr;
     graph_G = nullptr;
     graph_S = nullptr;
+    graph_sig.clear();
   }
+  // addresses of all device buffers a GW build reads or writes (capi.cu)
+  std::vector<const void*> buffer_signature() const;
   void invalidate() {
     gw_tables.reset();
     drop_graph();

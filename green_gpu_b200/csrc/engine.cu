@@ -153,6 +153,13 @@ void unfold_matrices(gg_context* c, const double2* X_in, int nouter, int ns, dou
   ++c->launches;
 }
 
+std::vector<int> shard_q_points(int inq, int rank, int size) {
+  if (size < 1 || rank < 0 || rank >= size || inq < 0) throw Error(GG_ERR_ARG, "q shard: need 0 <= rank < size");
+  std::vector<int> q;
+  for (int iq = rank; iq < inq; iq += size) q.push_back(iq);
+  return q;
+}
+
 int gw_spins(const gg_context* c) { return c->x2c ? 4 : c->sh.ns; }
 int hf_spins(const gg_context* c) { return c->x2c ? 3 : c->sh.ns; }
 
@@ -400,8 +407,7 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
   const double pref = ns == 1 ? -2.0 : -1.0;
   // irreducible q points owned by this shard (round-robin, src/cugw_utils.cu:115), in
   // chunks of pl.qc consecutive owned points; qi indexes the chunk, iq = myq[q0 + qi]
-  std::vector<int> myq;
-  for (int iq = c->shard_rank; iq < s.inq; iq += c->shard_size) myq.push_back(iq);
+  const std::vector<int> myq = shard_q_points(s.inq, c->shard_rank, c->shard_size);
   const int nmy = (int)myq.size();
   for (int q0 = 0; q0 < nmy; q0 += pl.qc) {
     const int qn = std::min(pl.qc, nmy - q0);

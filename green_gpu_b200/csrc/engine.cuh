@@ -8,6 +8,8 @@ namespace gg {
 Plan plan_gw(gg_context* c, int slices);
 // spin blocks the GW / HF engines loop over: ns, or the X2C pseudo-spins (4 for GW, 3 for HF)
 int gw_spins(const gg_context* c);
+// irreducible q points of shard `rank` of `size`: iq = rank, rank + size, ... (cugw_utils.cu:115)
+std::vector<int> shard_q_points(int inq, int rank, int size);
 int hf_spins(const gg_context* c);
 // X2C needs the identity k/q symmetry (no rotations, no time-reversal partners): the spinor
 // transformation of G under a space-group or time-reversal operation is not applied here

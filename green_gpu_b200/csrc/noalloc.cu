@@ -1,12 +1,15 @@
 // gg_zgemm_noalloc: the FP64 complex GEMM with its split-K scratch in a static device array.
 //
 // Who needs it: programs that are not allowed to allocate device memory at the point where
-// they want a contraction - code that runs while a CUDA graph is being captured, services
-// whose device memory is owned by another allocator (a caching pool that must not be
-// bypassed, or a memory budget fixed at start-up), and latency-critical loops where
-// cudaMalloc / cudaFree would synchronise the device and stall other streams.  They pass
-// device buffers for A, B and C; everything else this entry point needs lives in
-// `g_noalloc_scratch`, which every GPU that loads the library keeps until the process exits.
+// they want a contraction - services whose device memory is owned by another allocator (a
+// caching pool that must not be bypassed, or a memory budget fixed at start-up), and
+// latency-critical loops where cudaMalloc / cudaFree would synchronise the device and stall
+// other streams.  They pass device buffers for A, B and C; everything else this entry point
+// needs lives in `g_noalloc_scratch`, which every GPU that loads the library keeps until the
+// process exits.  The array's device address is looked up once per device, on the first
+// call there (cudaGetSymbolAddress with that device current); a cudaDeviceReset discards the
+// module and with it that address, so the entry point must not be called again on a device
+// that was reset in the same process.
 #include <mutex>
 
 #include "common.cuh"
@@ -18,15 +21,12 @@ namespace {
 constexpr long kScratchElems = 1L << 20;
 static __device__ __align__(256) double2 g_noalloc_scratch[kScratchElems];
 
-constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-double2* g_scratch_ptr[kMaxDevices] = {};
+double2* g_scratch_ptr[gg::kMaxDevices] = {};
 
 // device address of the scratch on the current device, looked up once per device
 double2* scratch_for_current_device() {
-  int dev = 0;
-  GG_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) throw gg::Error(GG_ERR_ARG, "zgemm_noalloc: device index out of range");
+  const int dev = gg::current_device();
   std::lock_guard<std::mutex> lock(g_mu);
   if (!g_scratch_ptr[dev]) {
     double2* p = nullptr;

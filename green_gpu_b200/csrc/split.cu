@@ -31,6 +31,7 @@
 #include <cuda.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 
@@ -756,23 +757,17 @@ CUtensorMap make_map(const int8_t* base, long rows_pad, long planes, int box_row
   return m;
 }
 
-int sms() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
-    GG_CUDA(cudaGetDevice(&dev));
-    GG_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
-  }
-  return n;
-}
+int sms() { return device_sm_count(); }
 
 template <int S, int BN>
 void launch_i8(const CUtensorMap& ta, const CUtensorMap& tb, const I8Args& a, long blocks, size_t smem,
                cudaStream_t st) {
-  static bool cfg = false;
-  if (!cfg) {
+  // the shared-memory attribute is per device: set once on each
+  static std::atomic<bool> cfg[kMaxDevices];
+  const int dev = current_device();
+  if (!cfg[dev].load(std::memory_order_acquire)) {
     GG_CUDA(cudaFuncSetAttribute(i8_gemm_kernel<S, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448));
-    cfg = true;
+    cfg[dev].store(true, std::memory_order_release);
   }
   i8_gemm_kernel<S, BN><<<(unsigned)blocks, NTHREADS, smem, st>>>(ta, tb, a);
   GG_CHECK_LAUNCH();
@@ -813,6 +808,14 @@ SplitGemm* split_engine(gg_context* c) {
 }
 
 void split_release(SplitGemm* e) { delete e; }
+
+void split_buffers(const SplitGemm* e, std::vector<const void*>& out) {
+  if (!e) {
+    out.push_back(nullptr);
+    return;
+  }
+  out.insert(out.end(), {e->a8.p, e->b8.p, e->ea.p, e->eb.p, e->err.p, e->work.p});
+}
 
 int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
   if (S < 2 || S > 8) throw Error(GG_ERR_ARG, "split: slices must be in [2, 8]");

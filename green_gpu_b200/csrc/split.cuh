@@ -12,6 +12,9 @@ SplitGemm* split_engine(gg_context* c);
 // Same contract as zgemm() for descriptors with KB >= 1; FP64 in, FP64 out.
 int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int slices, cudaStream_t st);
 void split_release(SplitGemm* e);
+// Device addresses of the engine's work buffers (appended to `out`): a graph that captured
+// split GEMMs stays valid only while none of them was reallocated.
+void split_buffers(const SplitGemm* e, std::vector<const void*>& out);
 // Raise if any split GEMM enqueued on `st` since the last check timed out (synchronises `st`).
 void split_check(SplitGemm* e, cudaStream_t st);
 

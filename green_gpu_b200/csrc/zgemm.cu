@@ -10,6 +10,8 @@
 // copies and the fragment loads are bank-conflict free without padding.
 #include "zgemm.cuh"
 
+#include <atomic>
+
 #include <algorithm>
 
 namespace gg {
@@ -542,17 +544,27 @@ void launch8_any(const ZgemmDesc& d, int tiles_m, int tiles_n, int span, int spa
   else launch8_layout<G3, false>(d, tiles_m, tiles_n, span, span_m, blocks, stream);
 }
 
-int sm_count() {
-  static int n = 0;
+int sm_count() { return device_sm_count(); }
+
+}  // namespace
+
+int current_device() {
+  int dev = 0;
+  GG_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) throw Error(GG_ERR_ARG, "device index " + std::to_string(dev) + " out of range");
+  return dev;
+}
+
+int device_sm_count() {
+  static std::atomic<int> counts[kMaxDevices];
+  const int dev = current_device();
+  int n = counts[dev].load(std::memory_order_relaxed);
   if (!n) {
-    int dev = 0;
-    GG_CUDA(cudaGetDevice(&dev));
     GG_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    counts[dev].store(n, std::memory_order_relaxed);
   }
   return n;
 }
-
-}  // namespace
 
 int zgemm(const ZgemmDesc& d0, cudaStream_t stream) {
   ZgemmDesc d = d0;

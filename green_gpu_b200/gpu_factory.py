@@ -39,7 +39,7 @@ def custom_kernel_parameters(p: dict) -> None:
     # B200-specific: split-precision contractions (replaces P_sp / Sigma_sp single precision)
     p.setdefault("P_sp", False)
     p.setdefault("Sigma_sp", False)
-    p.setdefault("split_slices", 4)
+    p.setdefault("split_slices", native.DEFAULT_SPLIT_SLICES)
 
 
 def _coulomb(p, key_mem, key_file, bz_utils, nao, NQ):
@@ -106,7 +106,7 @@ class scalar_gw_gpu_kernel:
         V = _coulomb(p, "dfintegral", "dfintegral_file", bz_utils, nao, NQ)
         self._ctx = _context(p, nao, ns, NQ, bz_utils, nts=nts, nw_b=nw_b, V=V)
         self._ctx.set_ir(ft.Ttn_FB, ft.Tnt_BF)
-        self._ctx.set_split_slices(int(p.get("split_slices", 4)))
+        self._ctx.set_split_slices(int(p.get("split_slices", native.DEFAULT_SPLIT_SLICES)))
 
     def solve(self, g, sigma):
         """Overwrite sigma [nts][ns][ink][nso][nso] with Sigma(tau) for G(tau) g."""

@@ -25,6 +25,8 @@ SOLVER_CHOLESKY = 0
 SOLVER_LU = 1
 PREC_FP64 = 0
 PREC_SPLIT = 1
+# slice count of GG_PREC_SPLIT unless set (GG_DEFAULT_SPLIT_SLICES in include/green_b200.h)
+DEFAULT_SPLIT_SLICES = 5
 
 EXPORTS = [
     "gg_create", "gg_destroy", "gg_last_error", "gg_set_symmetry", "gg_set_kpairs", "gg_set_coulomb",
@@ -32,7 +34,7 @@ EXPORTS = [
     "gg_set_capture", "gg_hf_exchange", "gg_hf_fock", "gg_symmetry_unfold", "gg_last_timings", "gg_version",
     "gg_set_profiling", "gg_kernel_stats", "gg_last_launch_count", "gg_set_q_shard", "gg_zgemm",
     "gg_zgemm_noalloc", "gg_set_hf_precision", "gg_estimate_bytes", "gg_set_x2c", "gg_set_graph",
-    "gg_batch_create", "gg_batch_run", "gg_batch_destroy",
+    "gg_batch_create", "gg_batch_run", "gg_batch_destroy", "gg_q_shard_points",
 ]
 
 
@@ -92,6 +94,8 @@ def load(path: str = LIB_PATH):
         "gg_batch_run": (C.c_int, [P, P]),
         "gg_batch_destroy": (None, [P]),
         "gg_estimate_bytes": (C.c_int, [C.POINTER(Shape), C.c_int64, C.POINTER(C.c_int64)]),
+        "gg_q_shard_points": (C.c_int, [C.c_int32, C.c_int, C.c_int, C.POINTER(C.c_int32), C.c_int32,
+                                        C.POINTER(C.c_int32)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -283,6 +287,17 @@ class Context:
         n = self.lib.gg_last_timings(self.h, _d(buf), 8)
         keys = ["total", "unfold", "p0", "ir_fwd", "dyson", "ir_back", "sigma", "e2e"]
         return dict(zip(keys[:n], buf[:n].tolist()))
+
+
+def q_shard_points(inq: int, rank: int, size: int) -> list:
+    """Irreducible q points of one shard, from the library (host-only; no device needed)."""
+    lib = load()
+    buf = (C.c_int32 * max(inq, 1))()
+    n = C.c_int32(0)
+    rc = lib.gg_q_shard_points(int(inq), int(rank), int(size), buf, max(inq, 1), C.byref(n))
+    if rc != GG_OK:
+        raise GreenError(rc, lib.gg_last_error(None).decode())
+    return [int(buf[i]) for i in range(n.value)]
 
 
 def estimate_bytes(nk, ink, inq, nao, NQ, ns, nts, nw_b, num_kpair_stored) -> int:

@@ -18,7 +18,7 @@ def main(argv=None):
     ap.add_argument("--nao", type=int, default=52)
     ap.add_argument("--NQ", type=int, default=400)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
-    ap.add_argument("--slices", type=int, default=4)
+    ap.add_argument("--slices", type=int, default=5)
     ap.add_argument("--repeat", type=int, default=1)
     a = ap.parse_args(argv)
     mesh = tuple(int(x) for x in a.mesh.split(","))

@@ -60,6 +60,7 @@ extern "C" {
 /* arithmetic of the contractions */
 #define GG_PREC_FP64 0     /* plain FP64 everywhere */
 #define GG_PREC_SPLIT 1    /* Ozaki-sliced INT8 tensor-core contractions, FP64 solve / IR / sums */
+#define GG_DEFAULT_SPLIT_SLICES 5
 
 typedef struct gg_context gg_context;
 
@@ -113,8 +114,15 @@ int gg_set_ir(gg_context* ctx, const double* Ttn_FB, const double* Tnt_BF);
  * round-robin distribution of src/cugw_utils.cu:115); the caller sums the partial Sigma
  * over ranks (src/gw_gpu_kernel.cpp:187).  (0, 1) restores the full build. */
 int gg_set_q_shard(gg_context* ctx, int rank, int size);
+/* The irreducible q points a shard owns (ascending), as gg_set_q_shard restricts a build to
+ * them: writes at most `capacity` indices to q_out and their number to count.  Host-only (no
+ * device, no context), so multi-rank drivers can plan the distribution before any GPU work. */
+int gg_q_shard_points(int32_t inq, int rank, int size, int32_t* q_out, int32_t capacity, int32_t* count);
 
-/* Number of Ozaki slices per operand for GG_PREC_SPLIT (2..8, default 4). */
+/* Number of Ozaki slices per operand for GG_PREC_SPLIT (2..8, default GG_DEFAULT_SPLIT_SLICES).
+ * Five slices is the smallest count that keeps Sigma, P0, the exchange K and the energies
+ * within 1e-8 relative of the FP64 path on the benchmark systems (four slices gives about
+ * 5e-8). */
 int gg_set_split_slices(gg_context* ctx, int slices);
 
 /* One GW self-energy build.  G_tskij complex [nts][ns][ink][nao][nao] (host), Sigma_tskij
@@ -206,15 +214,16 @@ int gg_zgemm(gg_context* ctx, int64_t M, int64_t N, int64_t K, const double* A, 
 /* C = A B for device buffers A [M][K], B [K][N], C [M][N] (row-major complex128, 16-byte
  * aligned), FP64 tensor-core engine, enqueued on `stream` (a cudaStream_t; NULL = legacy
  * default stream) without synchronising.  No counterpart in the reference: this entry
- * point exists for callers that may not allocate device memory where they call it - code
- * running while a CUDA graph is captured, programs whose device memory belongs to another
- * allocator or to a budget fixed at start-up, and latency-bound loops in which cudaMalloc's
- * implicit device synchronisation would stall other streams.  It allocates nothing: the
+ * point exists for callers that may not allocate device memory where they call it -
+ * programs whose device memory belongs to another allocator or to a budget fixed at
+ * start-up, and latency-bound loops in which cudaMalloc's implicit device synchronisation
+ * would stall other streams.  It allocates nothing: the
  * split-K partial sums live in a static 16 MiB device array (2^20 complex numbers) that
  * every GPU loading this library keeps until the process exits, so M * N may not exceed
  * 2^19 (larger sizes return GG_ERR_ARG with the limit in gg_last_error(NULL)).  The first
  * call on each device looks the array's address up once (cudaGetSymbolAddress with that
- * device current); make that first call before any stream capture.  All calls share the
+ * device current); make that first call before any stream capture, and do not call it again
+ * on a device after a cudaDeviceReset in the same process.  All calls share the
  * array and every value a call reads from it was written earlier in the same call, so
  * nothing needs clearing - but calls that overlap on the GPU (different streams, or
  * different host threads on one device) race on it and must be serialised by the caller. */

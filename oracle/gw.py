@@ -41,9 +41,12 @@ def p0_pair(V, G1, G0m, pref):
     P0[t][Q'][Q]    = pref sum_{ab} X2[Q][ab] X1[ab][Q']  (cugw_qkpt.cu:225)
     """
     NQ, n, _ = V.shape
-    A = np.einsum("tap,Qpb->tQab", G0m, V, optimize=True).reshape(len(G1), NQ, n * n)
-    Vc = np.conj(V)
-    B = np.einsum("Qal,tbl->tQab", Vc, G1, optimize=True).reshape(len(G1), NQ, n * n)
+    nt = len(G1)
+    # every contraction is a BLAS matmul: A[t] = G0m[t] @ V_(p, Q b), B[t] = conj(V)_(Q a, l) @ G1[t]^T
+    Vp = np.ascontiguousarray(V.transpose(1, 0, 2)).reshape(n, NQ * n)  # [p][(Q, b)]
+    A = np.matmul(G0m, Vp).reshape(nt, n, NQ, n).transpose(0, 2, 1, 3).reshape(nt, NQ, n * n)
+    Vc = np.conj(V).reshape(NQ * n, n)  # [(Q, a)][l]
+    B = np.matmul(Vc, np.swapaxes(G1, 1, 2)).reshape(nt, NQ, n * n)  # [t][Q][(a, b)]
     return pref * np.matmul(A, np.swapaxes(B, 1, 2))
 
 
@@ -130,9 +133,16 @@ def sigma_pair(V, G1, Wt, ns_pref=-1.0):
     Y2[t][(j,c)][Q] = sum_P W[t][P][Q] Y1[t][P][j][c]   (cugw_qkpt.cu:322; row-major W)
     Sigma[t][j][i] = -sum_{c,Q} Y2[t][(j,c)][Q] conj(V^Q_{ic})  (cugw_qkpt.cu:329)
     """
-    Y1 = np.einsum("Qjl,tlc->tQjc", V, G1, optimize=True)
-    Y2 = np.einsum("tPQ,tPjc->tQjc", Wt, Y1, optimize=True)
-    return ns_pref * np.einsum("tQjc,Qic->tji", Y2, np.conj(V), optimize=True)
+    NQ, n, _ = V.shape
+    nt = len(G1)
+    # the three contractions as BLAS matmuls (an einsum with a shared batch index does not
+    # reach BLAS): Y1[t] = V_(Q j, l) @ G1[t]; Y2[t] = W[t]^T @ Y1[t]_(P, j c);
+    # Sigma[t] = Y2[t]_(j, Q c) @ conj(V)_(Q c, i)
+    Y1 = np.matmul(V.reshape(NQ * n, n), G1).reshape(nt, NQ, n * n)
+    Y2 = np.matmul(np.swapaxes(Wt, 1, 2), Y1).reshape(nt, NQ, n, n)
+    Y2 = np.ascontiguousarray(Y2.transpose(0, 2, 1, 3)).reshape(nt, n, NQ * n)
+    Vh = np.ascontiguousarray(np.conj(V).transpose(0, 2, 1)).reshape(NQ * n, n)  # [(Q, c)][i]
+    return ns_pref * np.matmul(Y2, Vh)
 
 
 def rotate_w(sys_, Wt, q_deg):

@@ -59,3 +59,20 @@ def test_bad_shape_rejected_before_device_use(lib):
     with pytest.raises(native.GreenError) as e:
         native.Context(2, 2, 2, 2, 4, 1, 5, 3)
     assert e.value.code == native.GG_ERR_ARG
+
+
+def test_split_slice_default_is_the_same_everywhere():
+    # library default, Python binding and both plugin mirrors agree on five slices: the smallest
+    # count that keeps Sigma, P0 and K within 1e-8 of FP64 (four gives ~5e-8)
+    txt = open(os.path.join(ROOT, "include", "green_b200.h")).read()
+    m = re.search(r"#define\s+GG_DEFAULT_SPLIT_SLICES\s+(\d+)", txt)
+    assert m and int(m.group(1)) == 5
+    ctx_src = open(os.path.join(ROOT, "green_gpu_b200", "csrc", "context.cuh")).read()
+    assert "int slices = GG_DEFAULT_SPLIT_SLICES;" in ctx_src
+    from green_gpu_b200 import gpu_factory, native
+    assert native.DEFAULT_SPLIT_SLICES == 5
+    p = {}
+    gpu_factory.custom_kernel_parameters(p)
+    assert p["split_slices"] == 5
+    drop_in = open(os.path.join(ROOT, "include", "green", "gpu", "gpu_factory.h")).read()
+    assert "set_split_slices(GG_DEFAULT_SPLIT_SLICES)" in drop_in

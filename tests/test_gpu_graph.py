@@ -110,3 +110,49 @@ def test_batch_of_uneven_systems_in_one_graph(precision):
     batch.close()
     for ctx in ctxs:
         ctx.close()
+
+
+def test_graph_is_recaptured_after_other_entry_points_grow_shared_buffers():
+    # the HF exchange, the symmetry unfold and the split GEMM share the context's work buffers
+    # with the GW build; when they grow one, the captured graph would address freed memory, so
+    # the next build must capture again instead of replaying
+    s = tiny("tr", ns=1, seed=13)
+    ctx = native.context_for(s)
+    ctx.set_graph(True)
+    a = ctx.gw_sigma(s.G_tskij, precision=native.PREC_SPLIT)  # eager build, then capture
+    assert np.array_equal(ctx.gw_sigma(s.G_tskij, precision=native.PREC_SPLIT), a)  # replay
+    big = np.repeat(s.G_tskij[:, 0], 40, axis=0)  # [40 nts][ink][nao][nao]: grows the unfold scratch
+    ctx.symmetry_unfold(big)
+    ctx.set_hf_precision(native.PREC_SPLIT)
+    ctx.hf_exchange(s.dm)
+    rng = np.random.default_rng(1)
+    A = rng.standard_normal((700, 3000)) + 1j * rng.standard_normal((700, 3000))
+    ctx.zgemm(A, A.T.copy(), precision=native.PREC_SPLIT)     # grows the split engine's planes
+    b = ctx.gw_sigma(s.G_tskij, precision=native.PREC_SPLIT)  # eager again, captured again
+    c = ctx.gw_sigma(s.G_tskij, precision=native.PREC_SPLIT)  # replay of the new graph
+    assert np.array_equal(b, a)
+    assert np.array_equal(c, a)
+    ctx.close()
+
+
+def test_batch_refuses_to_replay_after_a_member_context_changed():
+    systems = [tiny("tr", ns=1, seed=14), tiny("none", ns=1, seed=15, mesh=(2, 1, 1), nao=6, NQ=20)]
+    dev = torch.device("cuda:0")
+    items, ctxs, bufs = [], [], []
+    for s in systems:
+        ctx = native.context_for(s)
+        G = torch.from_numpy(s.G_tskij.view(np.float64)).to(dev)
+        S = torch.zeros_like(G)
+        bufs.append((G, S))
+        ctxs.append(ctx)
+        items.append((ctx, G.data_ptr(), S.data_ptr()))
+    batch = native.Batch(items)
+    batch.run()
+    big = np.repeat(systems[0].G_tskij[:, 0], 40, axis=0)
+    ctxs[0].symmetry_unfold(big)                              # reallocates a buffer the graph uses
+    with pytest.raises(native.GreenError) as e:
+        batch.run()
+    assert e.value.code == native.GG_ERR_STATE
+    batch.close()
+    for ctx in ctxs:
+        ctx.close()

@@ -27,7 +27,10 @@ def _worker(rank, world, port, out):
     from oracle import gw as ogw
     s = synth.make_system(mesh=(3, 2, 1), nao=4, NQ=10, ns=1, beta=10.0, lam=100.0, nts=24, nw_b=21, seed=1,
                           symmetry="tr")
-    mine = list(range(rank, s.inq, world))
+    # the library's own shard assignment (host-side, callable without a GPU)
+    from green_gpu_b200 import native
+    mine = native.q_shard_points(s.inq, rank, world)
+    assert mine == list(range(rank, s.inq, world))
     part = ogw.gw_build(s, q_subset=mine)
     t = torch.from_numpy(part.view(np.float64).copy())
     dist.all_reduce(t)
@@ -50,7 +53,11 @@ def test_q_sharded_sigma_sums_to_full(tmp_path):
 
 
 def test_round_robin_partition_covers_every_q_once():
+    from green_gpu_b200 import native
     for inq in (1, 4, 7, 64):
         for world in (1, 2, 3, 8):
-            seen = sorted(q for r in range(world) for q in range(r, inq, world))
+            seen = sorted(q for r in range(world) for q in native.q_shard_points(inq, r, world))
             assert seen == list(range(inq))
+    import pytest
+    with pytest.raises(native.GreenError):
+        native.q_shard_points(4, 2, 2)

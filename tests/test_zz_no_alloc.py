@@ -1,12 +1,12 @@
 """The allocation-free GEMM entry point (gg_zgemm_noalloc).
 
 Some callers may not allocate device memory at the point where they need a contraction:
-code running while a CUDA graph is being captured, services whose device memory is owned
-by another allocator or fixed at start-up, and latency-bound loops where cudaMalloc's
-implicit synchronisation would stall other streams.  gg_zgemm_noalloc serves them with
-caller-owned device buffers for A, B and C and a static device scratch array for its
-split-K partial sums.  These tests call it through the C ABI twice in a row and compare it
-with the allocating gg_zgemm entry point; they run last (file name) and also pass alone.
+services whose device memory is owned by another allocator or fixed at start-up, and
+latency-bound loops where cudaMalloc's implicit synchronisation would stall other streams.
+gg_zgemm_noalloc serves them with caller-owned device buffers for A, B and C and a static
+device scratch array for its split-K partial sums.  These tests call it through the C ABI
+twice in a row and compare it with the allocating gg_zgemm entry point and with A @ B in
+numpy (1e-13 of the largest element); they run last (file name) and also pass alone.
 """
 import ctypes
 
@@ -49,6 +49,8 @@ def test_noalloc_gemm_matches_allocating_entry_point_twice():
         got = _noalloc(lib, A, B)
         want = ctx.zgemm(A, B, precision=native.PREC_FP64)
         assert np.abs(got - want).max() <= 1e-13 * np.abs(want).max()
+        ref = A @ B
+        assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
     ctx.close()
 
 
