@@ -85,7 +85,18 @@ class IRBasis:
     """
 
     def __init__(self, beta: float = 100.0, lam: float = 1e4, nts: int = 72, nw_b: int = 69,
-                 order: int = 24):
+                 order: int = 24, tau=None):
+        """``tau`` (optional): a given grid of nts points, 0 and beta included and symmetric
+        under tau -> beta - tau (for example the sampling points of an IR basis file, which
+        come from an extended-precision expansion beyond the reach of this double-precision
+        SVD); the transforms are then built on it instead of on roots of u_{nts-2}."""
+        if tau is not None:
+            tau = np.asarray(tau, dtype=np.float64)
+            nts = len(tau)
+            if tau[0] != 0.0 or tau[-1] != beta or np.any(np.diff(tau) <= 0):
+                raise ValueError("tau must rise from 0 to beta")
+            if np.abs(tau + tau[::-1] - beta).max() > 1e-6 * beta:
+                raise ValueError("tau must be symmetric under tau -> beta - tau")
         if nts % 2:
             raise ValueError("nts must be even (tau grid symmetric about beta/2)")
         if nw_b > nts - 2:
@@ -113,6 +124,10 @@ class IRBasis:
         self._V = Vt.T
         L = nts - 2
         self.L = L
+        if tau is not None:
+            self.tau = tau.copy()
+            self._finish(tau[1:-1], nw_b, lam)
+            return
         # sampling times: interior roots of u_L (the (L+1)-th singular function)
         dense = np.unique(np.concatenate([np.linspace(0, beta / 2, 20001)[1:],
                                           np.geomspace(1e-7 * beta, beta / 2, 20001)]))
@@ -139,6 +154,9 @@ class IRBasis:
         roots = roots[:need] if len(roots) == need else roots[np.linspace(0, len(roots) - 1, need).round().astype(int)]
         interior = np.concatenate([roots, beta - roots[::-1]])
         self.tau = np.concatenate([[0.0], interior, [beta]])
+        self._finish(interior, nw_b, lam)
+
+    def _finish(self, interior, nw_b, lam):
         # bosonic frequencies: a set symmetric under n -> -n (n = 0 included when nw_b is
         # odd), so that the transform pair commutes with complex conjugation exactly as
         # the physical Fourier transform of a tau-symmetric function does.  Pairs are
@@ -180,6 +198,13 @@ class IRBasis:
 
 
 _CACHE: dict = {}
+
+
+def ir_matrices_on_grid(tau, beta: float = 100.0, lam: float = 1e4, nw_b: int = 81):
+    """(Ttn_FB, Tnt_BF) on a given tau grid (0 and beta included, symmetric), nw_b bosonic
+    basis functions fitted on its interior points."""
+    b = IRBasis(beta, lam, len(tau), nw_b, tau=tau)
+    return b.Ttn_FB.copy(), b.Tnt_BF.copy()
 
 
 def ir_matrices(beta: float = 100.0, lam: float = 1e4, nts: int = 72, nw_b: int = 69):

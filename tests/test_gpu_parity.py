@@ -123,3 +123,23 @@ def test_missing_inputs_are_reported():
     with pytest.raises(native.GreenError) as e:
         ctx.gw_sigma(s.G_tskij)
     assert e.value.code == native.GG_ERR_STATE
+
+
+@pytest.mark.parametrize("precision,solver", [(native.PREC_FP64, native.SOLVER_LU),
+                                              (native.PREC_FP64, native.SOLVER_CHOLESKY),
+                                              (native.PREC_SPLIT, native.SOLVER_LU)])
+def test_gw_matches_reference_sigma_tau(precision, solver):
+    # test/cu_solver_test.cpp:226-288 (solve_gw, GW_LU / GW_Cholesky sections): one GW
+    # iteration of the H2 27 -> 4 k fixture with space-group rotations, result/Sigma_tau at
+    # |a - b| < 1e-6 (:287), on transforms built on the fixture's recovered tau grid
+    # (tests/golden/gw_grid.py); split precision at the library's default slice count
+    import gw_grid
+    _, Ttn, Tnt = gw_grid.fixture_transforms()
+    s, ref = fixture.load(gw=True)
+    s.nw_b, s.Ttn_FB, s.Tnt_BF = Ttn.shape[1], Ttn, Tnt
+    ctx = native.context_for(s)
+    out = ctx.gw_sigma(s.G_tskij, solver=solver, precision=precision)
+    assert np.abs(out - ref["Sigma_tau_gw"]).max() < 1e-6
+    if precision == native.PREC_FP64:
+        assert rel(out, ogw.gw_build(s, solver="lu" if solver == native.SOLVER_LU else "cholesky")) < TOL_FP64
+    ctx.close()
