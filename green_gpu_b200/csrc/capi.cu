@@ -6,6 +6,7 @@
 #include <memory>
 #include <vector>
 
+#include "abi.cuh"
 #include "context.cuh"
 #include "engine.cuh"
 #include "kernels.cuh"
@@ -18,25 +19,6 @@ namespace {
 
 thread_local std::string g_create_error;
 
-template <typename F>
-int guarded(gg_context* c, F&& f) {
-  if (!c) return GG_ERR_ARG;
-  try {
-    GG_CUDA(cudaSetDevice(c->device));
-    f();
-    c->err.clear();
-    return GG_OK;
-  } catch (const Error& e) {
-    c->err = e.what();
-    return e.code;
-  } catch (const std::exception& e) {
-    c->err = e.what();
-    return GG_ERR_INTERNAL;
-  } catch (...) {
-    c->err = "unknown error";
-    return GG_ERR_INTERNAL;
-  }
-}
 
 void check_shape(const gg_shape& s) {
   auto bad = [](const std::string& m) { throw Error(GG_ERR_ARG, "shape: " + m); };
@@ -53,19 +35,6 @@ void check_shape(const gg_shape& s) {
 
 void gg::set_thread_error(const std::string& msg) { g_create_error = msg; }
 
-template <typename F>
-static int guarded_global(F&& f) {
-  try {
-    f();
-    return GG_OK;
-  } catch (const Error& e) {
-    gg::set_thread_error(e.what());
-    return e.code;
-  } catch (const std::exception& e) {
-    gg::set_thread_error(e.what());
-    return GG_ERR_INTERNAL;
-  }
-}
 
 extern "C" {
 

@@ -79,6 +79,23 @@ __global__ void gather_blocks_kernel(const double2* __restrict__ src, const int*
   }
 }
 
+__global__ void transpose_blocks_kernel(const double2* __restrict__ in, int n, int tiles, double2* __restrict__ out) {
+  __shared__ double2 t[32][33];
+  const long b = blockIdx.y;
+  const int ti = blockIdx.x / tiles, tj = blockIdx.x % tiles;
+  const double2* src = in + b * (long)n * n;
+  double2* dst = out + b * (long)n * n;
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int i = ti * 32 + r, j = tj * 32 + threadIdx.x;
+    if (i < n && j < n) t[r][threadIdx.x] = src[(long)i * n + j];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int j = tj * 32 + r, i = ti * 32 + threadIdx.x;
+    if (i < n && j < n) dst[(long)j * n + i] = t[threadIdx.x][r];
+  }
+}
+
 __global__ void axpy_kernel(double2* y, const double2* x, long n) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
     y[i] = cadd(y[i], x[i]);
@@ -566,6 +583,14 @@ __global__ void info_collect_kernel(const int* info, int count, int base, int* e
 
 void launch_info_collect(const int* info, int count, int base, int* err, cudaStream_t st) {
   info_collect_kernel<<<grid_for(count), TPB, 0, st>>>(info, count, base, err);
+  GG_CHECK_LAUNCH();
+}
+
+void launch_transpose_blocks(const double2* in, long nblocks, int n, double2* out, cudaStream_t st) {
+  if (nblocks <= 0 || n <= 0) return;
+  if (nblocks > 65535) throw Error(GG_ERR_ARG, "transpose: too many blocks for one launch");
+  const int tiles = (n + 31) / 32;
+  transpose_blocks_kernel<<<dim3((unsigned)(tiles * tiles), (unsigned)nblocks), dim3(32, 8), 0, st>>>(in, n, tiles, out);
   GG_CHECK_LAUNCH();
 }
 

@@ -37,6 +37,9 @@ void launch_x2c_split(const double2* in, long nouter, long ninner, int n, int nb
 // block is the adjoint of ab (cuda_common.cu:176-201)
 void launch_x2c_merge(const double2* in, long nouter, long ninner, int n, int nblk, double2* out, cudaStream_t st);
 
+// out[b][i][j] = in[b][j][i] for nblocks n x n matrices (32 x 32 tiles through shared memory)
+void launch_transpose_blocks(const double2* in, long nblocks, int n, double2* out, cudaStream_t st);
+
 // scale: X *= s
 void launch_scale(double2* X, long n, double s, cudaStream_t st);
 void launch_fill_zero(double2* X, long n, cudaStream_t st);

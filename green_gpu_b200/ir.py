@@ -120,6 +120,7 @@ class IRBasis:
         M = np.sqrt(tw)[:, None] * K * np.sqrt(ww)[None, :]
         U, s, Vt = np.linalg.svd(M, full_matrices=False)
         self._wx, self._ww = wx, ww
+        self._tx, self._tw = tx, tw
         self._s = s
         self._V = Vt.T
         L = nts - 2
@@ -195,6 +196,27 @@ class IRBasis:
         ls = list(ls)
         K = _kernel_iw(np.asarray(n), self._wx, self.beta)
         return (K * np.sqrt(self._ww)[None, :]) @ self._V[:, ls] / self._s[ls][None, :]
+
+
+def tau_quadrature(tau, beta: float = 100.0, lam: float = 1e4, nl=None, cutoff: float = 1e-13):
+    """Real matrix M [nts][nts] with int_0^beta f(tau) g(beta - tau) dtau = f^T M g for functions
+    f, g sampled on the grid `tau` (0 and beta included) and spanned by the first nl singular
+    functions u_l of the logistic kernel: M = Fit^T O Fit with Fit the least-squares fit of
+    the coefficients from the samples and O_ll' = int u_l(tau) u_l'(beta - tau) dtau (computed
+    on the kernel's own quadrature; (-1)^l delta_ll' for the exact functions).  By default nl
+    keeps the functions with s_l / s_0 > cutoff, at most nts - 2."""
+    tau = np.asarray(tau, dtype=np.float64)
+    nts = len(tau)
+    b = IRBasis(beta, lam, nts, 1, tau=tau)
+    if nl is None:
+        nl = int(min(nts - 2, np.count_nonzero(b._s / b._s[0] > cutoff)))
+    ls = range(nl)
+    U = b.u(tau, ls)
+    fit = np.linalg.pinv(U)
+    uq = b.u(b._tx, ls)
+    ur = b.u(beta - b._tx, ls)
+    O = (uq * b._tw[:, None]).T @ ur
+    return fit.T @ O @ fit
 
 
 _CACHE: dict = {}

@@ -34,7 +34,8 @@ EXPORTS = [
     "gg_set_capture", "gg_hf_exchange", "gg_hf_fock", "gg_symmetry_unfold", "gg_last_timings", "gg_version",
     "gg_set_profiling", "gg_kernel_stats", "gg_last_launch_count", "gg_set_q_shard", "gg_zgemm",
     "gg_zgemm_noalloc", "gg_set_hf_precision", "gg_estimate_bytes", "gg_set_x2c", "gg_set_graph",
-    "gg_batch_create", "gg_batch_run", "gg_batch_destroy", "gg_q_shard_points",
+    "gg_batch_create", "gg_batch_run", "gg_batch_destroy", "gg_q_shard_points", "gg_energy_hf", "gg_energy_gw",
+    "gg_energy_gw_device", "gg_chemical_potential",
 ]
 
 
@@ -96,6 +97,11 @@ def load(path: str = LIB_PATH):
         "gg_estimate_bytes": (C.c_int, [C.POINTER(Shape), C.c_int64, C.POINTER(C.c_int64)]),
         "gg_q_shard_points": (C.c_int, [C.c_int32, C.c_int, C.c_int, C.POINTER(C.c_int32), C.c_int32,
                                         C.POINTER(C.c_int32)]),
+        "gg_energy_hf": (C.c_int, [P, D, D, D, D]),
+        "gg_energy_gw": (C.c_int, [P, D, D, D, D]),
+        "gg_energy_gw_device": (C.c_int, [P, P, P, D, D, P]),
+        "gg_chemical_potential": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, D, D, D, C.c_double, C.c_double,
+                                            C.c_double, D, D]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -282,6 +288,28 @@ class Context:
                                       _d(out.view(np.float64)), int(precision)))
         return out
 
+    def energy_hf(self, dm, H, F):
+        """(E_1b, E_HF) in FP64 (gg_energy_hf)."""
+        out = np.zeros(2)
+        self._check(self.lib.gg_energy_hf(self.h, _d(_c128(dm).view(np.float64)), _d(_c128(H).view(np.float64)),
+                                          _d(_c128(F).view(np.float64)), _d(out)))
+        return float(out[0]), float(out[1])
+
+    def energy_gw(self, G_tskij, Sigma_tskij, M):
+        """Galitskii-Migdal E_GW in FP64 with the tau quadrature M (gg_energy_gw)."""
+        e = np.zeros(1)
+        Mq = np.ascontiguousarray(M, dtype=np.float64)
+        self._check(self.lib.gg_energy_gw(self.h, _d(_c128(G_tskij).view(np.float64)),
+                                          _d(_c128(Sigma_tskij).view(np.float64)), _d(Mq), _d(e)))
+        return float(e[0])
+
+    def energy_gw_device(self, G_ptr: int, Sigma_ptr: int, M, stream=0):
+        e = np.zeros(1)
+        Mq = np.ascontiguousarray(M, dtype=np.float64)
+        self._check(self.lib.gg_energy_gw_device(self.h, C.c_void_p(int(G_ptr)), C.c_void_p(int(Sigma_ptr)), _d(Mq),
+                                                 _d(e), C.c_void_p(int(stream))))
+        return float(e[0])
+
     def timings(self):
         buf = np.zeros(8)
         n = self.lib.gg_last_timings(self.h, _d(buf), 8)
@@ -298,6 +326,22 @@ def q_shard_points(inq: int, rank: int, size: int) -> list:
     if rc != GG_OK:
         raise GreenError(rc, lib.gg_last_error(None).decode())
     return [int(buf[i]) for i in range(n.value)]
+
+
+def chemical_potential(F, S, weights, beta, nelec, spin_factor):
+    """(mu, N(mu)) of a mean-field state (gg_chemical_potential; host-only, no device needed)."""
+    lib = load()
+    F = _c128(F)
+    S = _c128(S)
+    ns, ink, n = F.shape[0], F.shape[1], F.shape[-1]
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    mu = C.c_double(0.0)
+    nat = C.c_double(0.0)
+    rc = lib.gg_chemical_potential(ns, ink, n, _d(w), _d(F.view(np.float64)), _d(S.view(np.float64)), float(beta),
+                                   float(spin_factor), float(nelec), C.byref(mu), C.byref(nat))
+    if rc != GG_OK:
+        raise GreenError(rc, lib.gg_last_error(None).decode())
+    return mu.value, nat.value
 
 
 def estimate_bytes(nk, ink, inq, nao, NQ, ns, nts, nw_b, num_kpair_stored) -> int:

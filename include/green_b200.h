@@ -229,6 +229,33 @@ int gg_zgemm(gg_context* ctx, int64_t M, int64_t N, int64_t K, const double* A, 
  * different host threads on one device) race on it and must be serialised by the caller. */
 int gg_zgemm_noalloc(int64_t M, int64_t N, int64_t K, const void* A, const void* B, void* C, void* stream);
 
+/* FP64 energy and chemical-potential reductions.  green-gpu returns Sigma(tau) and the Fock
+ * matrix and leaves these reductions to its caller, green-mbpt (its GW / HF solvers read
+ * the kernels' outputs and reduce them in double precision); they are provided here so that a
+ * caller of this library keeps them in FP64 next to the data.  k weights are |star(k)| / nk
+ * from the context's symmetry tables; the spin factor f is 2 for ns = 1, 1 for ns = 2 and in
+ * X2C mode (where the matrices are the spinor ones).
+ *   gg_energy_hf: dm, H (one-body Hamiltonian) and F (Fock matrix) [ns][ink][m][m] host;
+ *     out[0] = E_1b = f sum_{s,k} w_k Re Tr(dm H), out[1] = E_HF = (f/2) sum w_k Re Tr(dm (H + F)).
+ *   gg_energy_gw[_device]: G and Sigma [nts][ns][ink][m][m] (host, or device buffers on
+ *     `stream`), M [nts][nts] real (host) a bilinear quadrature of
+ *     int_0^beta f(tau) g(beta - tau) dtau on the tau grid; *e_gw = -(f/2) sum_{s,k} w_k
+ *     sum_{t,t'} M[t][t'] Re Tr(Sigma(tau_t) G(tau_t')) (Galitskii-Migdal), traces on the FP64
+ *     tensor-core engine. */
+int gg_energy_hf(gg_context* ctx, const double* dm, const double* H, const double* F, double* out);
+int gg_energy_gw(gg_context* ctx, const double* G_tskij, const double* Sigma_tskij, const double* M,
+                 double* e_gw);
+int gg_energy_gw_device(gg_context* ctx, const void* G_tskij_device, const void* Sigma_tskij_device,
+                        const double* M, double* e_gw, void* stream);
+/* Chemical potential of a mean-field state: the mu with
+ * spin_factor sum_{s,k} weights[k] sum_n 1 / (1 + exp(beta (e_skn - mu))) = nelec, where e_skn
+ * are the eigenvalues of F_s(k) x = e S_s(k) x (F, S complex [ns][ink][n][n], host), found by a
+ * Cholesky reduction and cyclic Jacobi in FP64 and bisected to FP64 resolution.  *n_at_mu (may
+ * be NULL) receives the particle number at the result.  Host-only, context-free. */
+int gg_chemical_potential(int32_t ns, int32_t ink, int32_t n, const double* weights, const double* F,
+                          const double* S, double beta, double spin_factor, double nelec, double* mu,
+                          double* n_at_mu);
+
 /* Device bytes a context of this shape needs when its integrals are resident and its GW
  * work space is planned without chunking (V store of num_kpair_stored pairs + work space);
  * context-free, allocates nothing.  Used for admission by memory footprint. */
