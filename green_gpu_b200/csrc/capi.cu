@@ -609,6 +609,10 @@ int gg_symmetry_unfold(gg_context* c, const double* X_ibz, int64_t nmat, double*
   });
 }
 
+int gg_arm_split_timeout_test(gg_context* c) {
+  return guarded(c, [&] { split_arm_timeout_test(split_engine(c)); });
+}
+
 int gg_set_profiling(gg_context* c, int enable) {
   return guarded(c, [&] { c->profiling = enable != 0; });
 }

@@ -44,6 +44,7 @@ struct SplitGemm {
   DevBuf<int> ea, eb, err;
   DevBuf<double2> work;
   int err_host = 0;
+  bool timeout_test = false;  // the next launch runs the time-out test (one-shot)
 };
 
 namespace {
@@ -97,13 +98,13 @@ __device__ __forceinline__ bool mbar_try_sleep(uint64_t* b, uint32_t parity, uin
 }
 // bounded wait; returns false (and records `code`) on time-out or when another role failed
 // (abort_on_err = false for the teardown waits that must see in-flight work complete)
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* err, int code,
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* err, int code, long long limit,
                                           bool abort_on_err = true) {
   if (mbar_try(b, parity)) return true;  // fast path: no clock read when the phase is complete
   const long long t0 = clock64();
   while (!mbar_try_sleep(b, parity, 100000)) {  // <= 0.1 ms per suspension
     if (abort_on_err && *err) return false;
-    if (clock64() - t0 > WAIT_CYCLES) {
+    if (clock64() - t0 > limit) {
       atomicOr((int*)err, code);
       return false;
     }
@@ -221,6 +222,9 @@ struct I8Args {
   int nbuf;  // accumulator sets in TMEM (1 or 2)
   int a_shared, b_shared;  // operand identical for every batch: sliced once, planes / exponents of batch 0
   int* err;
+  long long wait_cycles;   // limit of every barrier wait (WAIT_CYCLES; shorter in the time-out test)
+  int skip_arrive;         // time-out test: CTA 0's first epilogue warp never releases the first
+                           // drained accumulator, so the MMA warp's wait for it must run out
 };
 
 struct Unit {
@@ -252,11 +256,11 @@ __device__ __forceinline__ Unit unit_of(const I8Args& p, long u, int BN) {
 template <int S, int BN, bool FIRST, bool LAST>
 __device__ __forceinline__ bool issue_kblock(uint32_t tacc0, uint64_t da, uint64_t db, uint32_t idesc, uint32_t leader,
                                              bool reuse, uint64_t* acce, uint64_t* accf, uint32_t par_e,
-                                             volatile int* err) {
+                                             volatile int* err, long long limit) {
 #pragma unroll
   for (int d = 2; d <= S + 1; ++d) {
     if (FIRST && reuse) {
-      if (!__all_sync(0xffffffffu, mbar_wait(&acce[d - 2], par_e, err, 2))) return false;
+      if (!__all_sync(0xffffffffu, mbar_wait(&acce[d - 2], par_e, err, 2, limit))) return false;
       tc_fence_after();
     }
     const uint32_t tacc = tacc0 + (uint32_t)((d - 2) * BN);
@@ -365,7 +369,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const int planeA0 = p.a_shared ? 0 : (int)(w.batch * S * p.nkb);
         const int planeB0 = p.b_shared ? 0 : (int)(w.batch * S * p.nkb);
         for (int kb = w.kb0; kb < w.kb1; ++kb, ++it) {
-          if (!__all_sync(0xffffffffu, mbar_wait(&empty[st], ph ^ 1, err, 1))) { ok = false; break; }
+          if (!__all_sync(0xffffffffu, mbar_wait(&empty[st], ph ^ 1, err, 1, p.wait_cycles))) { ok = false; break; }
           mbar_expect_tx(&full[st], (uint32_t)(stA + stB), leader);
 #pragma unroll
           for (int s = 0; s < S; ++s) {
@@ -378,10 +382,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           }
         }
       }
-      // on failure, let the copies already issued land before the CTA can exit
-      if (!ok)
-        for (long j = (it > p.stages ? it - p.stages : 0); j < it; ++j)
-          mbar_wait(&full[j % p.stages], (uint32_t)((j / p.stages) & 1), err, 16, false);
+      // let the copies already issued land before the CTA can exit: after a failure elsewhere
+      // (the MMA warp stops consuming, so the last stages may still be in flight) and, at no
+      // cost, after a normal run (those phases completed long ago)
+      for (long j = (it > p.stages ? it - p.stages : 0); j < it; ++j)
+        mbar_wait(&full[j % p.stages], (uint32_t)((j / p.stages) & 1), err, 16, p.wait_cycles, false);
+      (void)ok;
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer (whole warp, lane 0 issues)
@@ -405,7 +411,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           const bool last = (kb + 1 == w.kb1) || kin + 1 == p.kcb;
           const bool reuse = first && use > 0;
           const uint32_t par_e = (uint32_t)((use - 1) & 1);
-          if (!__all_sync(0xffffffffu, mbar_wait(&full[st], ph, err, 4))) { ok = false; break; }
+          if (!__all_sync(0xffffffffu, mbar_wait(&full[st], ph, err, 4, p.wait_cycles))) { ok = false; break; }
           tc_fence_after();
           const uint64_t da = dA0 + (uint64_t)((st * stA) >> 4);
           const uint64_t db = dB0 + (uint64_t)((st * stB) >> 4);
@@ -415,11 +421,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           if (!first && !last)
             issue_kblock_grouped<S, BN>(tacc0, da, db, idesc_nofield, leader);
           else if (first && !last)
-            ok = issue_kblock<S, BN, true, false>(tacc0, da, db, idesc, leader, reuse, ae, af, par_e, err);
+            ok = issue_kblock<S, BN, true, false>(tacc0, da, db, idesc, leader, reuse, ae, af, par_e, err, p.wait_cycles);
           else if (!first)
-            issue_kblock<S, BN, false, true>(tacc0, da, db, idesc, leader, false, ae, af, 0u, err);
+            issue_kblock<S, BN, false, true>(tacc0, da, db, idesc, leader, false, ae, af, 0u, err, p.wait_cycles);
           else
-            ok = issue_kblock<S, BN, true, true>(tacc0, da, db, idesc, leader, reuse, ae, af, par_e, err);
+            ok = issue_kblock<S, BN, true, true>(tacc0, da, db, idesc, leader, reuse, ae, af, par_e, err, p.wait_cycles);
           if (!ok) break;
           mma_commit(&empty[st], leader);
           if (++st == p.stages) {
@@ -435,7 +441,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       }
       // all MMAs issued by lane 0 complete before TMEM can be freed
       mma_commit(fin, leader);
-      mbar_wait(fin, 0, err, 32, false);
+      mbar_wait(fin, 0, err, 32, p.wait_cycles, false);
     }
   } else {
     // ---------------- epilogue: 8 warps, lanes 32*(warp%4).., column half (warp-2)/4
@@ -462,7 +468,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       for (int k0 = w.kb0; k0 < w.kb1 && ok; k0 = min(w.kb1, (k0 / p.kcb + 1) * p.kcb)) {
 #pragma unroll
         for (int d = 2; d <= S + 1; ++d) {
-          if (!mbar_wait(&accf[buf * ND + d - 2], par, err, 8)) { ok = false; break; }
+          if (!mbar_wait(&accf[buf * ND + d - 2], par, err, 8, p.wait_cycles)) { ok = false; break; }
           tc_fence_after();
           const double scale = __longlong_as_double((long long)(1023 - 7 * d) << 52);  // 2^-7d
           const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)buf * buf_cols +
@@ -473,7 +479,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           if constexpr (HC % 32 != 0) drain_cols<HC % 32>(base + (HC / 32) * 32, acc + (HC / 32) * 32, scale);
           tc_fence_before();
           __syncwarp();
-          if (lane == 0) mbar_arrive(&acce[buf * ND + d - 2]);
+          const bool withheld = p.skip_arrive && blockIdx.x == 0 && warp == 2 && u == blockIdx.x && d == 2;
+          if (lane == 0 && !withheld) mbar_arrive(&acce[buf * ND + d - 2]);
         }
         if (++buf == p.nbuf) {
           buf = 0;
@@ -809,6 +816,8 @@ SplitGemm* split_engine(gg_context* c) {
 
 void split_release(SplitGemm* e) { delete e; }
 
+void split_arm_timeout_test(SplitGemm* e) { e->timeout_test = true; }
+
 void split_buffers(const SplitGemm* e, std::vector<const void*>& out) {
   if (!e) {
     out.push_back(nullptr);
@@ -897,6 +906,15 @@ int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
   a.alpha = d.alpha;
   a.beta = d.beta;
   a.err = err;
+  a.wait_cycles = WAIT_CYCLES;
+  a.skip_arrive = 0;
+  if (e->timeout_test) {
+    // ~0.1 s limit, and CTA 0 withholds one accumulator release (its MMA warp waits for it in
+    // its second work unit: the launch needs more units than CTAs)
+    a.wait_cycles = 200000000LL;
+    a.skip_arrive = 1;
+    e->timeout_test = false;
+  }
   a.nbuf = nbuf;
   a.a_shared = a_shared ? 1 : 0;
   a.b_shared = b_shared ? 1 : 0;

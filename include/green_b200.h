@@ -261,6 +261,15 @@ int gg_chemical_potential(int32_t ns, int32_t ink, int32_t n, const double* weig
  * context-free, allocates nothing.  Used for admission by memory footprint. */
 int gg_estimate_bytes(const gg_shape* shape, int64_t num_kpair_stored, int64_t* bytes);
 
+/* Test hook of the split engine's time-out path (no counterpart in the reference, whose device
+ * lock spins without a limit: src/cuda_common.cu:225-231).  The next split-precision GEMM on
+ * this context runs with a 0.1 s limit on every barrier wait, and one epilogue warp of CTA 0
+ * withholds its release of the first accumulator it drains, so the MMA warp's wait for that
+ * accumulator runs out (the GEMM needs more work units than SMs).  The kernel records the
+ * time-out, waits (bounded) for its copies and MMAs in flight, frees its tensor memory and
+ * returns; the call reports GG_ERR_INTERNAL and the context stays usable.  One-shot. */
+int gg_arm_split_timeout_test(gg_context* ctx);
+
 /* Library build information string (static storage). */
 const char* gg_version(void);
 
