@@ -189,7 +189,7 @@ Plan plan_gw(gg_context* c, int slices) {
     b += 2 * (size_t)s.nk * nspin * s.nts * nn;       // Gf + Gtmp
     b += (size_t)q.kc * Nnn;                           // Vbuf
     b += (size_t)q.kc * T2 * nn;                       // G1buf
-    size_t p0s = (size_t)q.kc * q.tb * Nnn;            // A / B build buffers (each)
+    size_t p0s = slices > 0 ? 0 : (size_t)q.kc * q.tb * Nnn;  // FP64 A / B build buffers (each)
     size_t sgs = (size_t)s.nts * std::max(Nnn, NN);    // Sigma X / Z, W rotation (each)
     b += 2 * std::max(p0s, sgs);
     b += (size_t)q.qc * T2 * NN;                       // P0
@@ -245,6 +245,119 @@ void dyson_failure(const gg_context* c, int solver, int system, int info) {
                   (solver == GG_SOLVER_CHOLESKY ? "positive definite" : "invertible"));
 }
 
+namespace {
+
+// C^T = B^T A^T as a descriptor: the INT8 engine's epilogue gives each lane one row of C, so
+// the operand builds (outputs contiguous along n) are computed transposed for coalesced stores
+ZgemmDesc transposed(const ZgemmDesc& d) {
+  ZgemmDesc t = d;
+  t.M = d.N; t.N = d.M;
+  t.A = d.B; t.a_m = d.b_n; t.a_k = d.b_k; t.a_kb = d.b_kb; t.conjA = d.conjB;
+  t.a_b0 = d.b_b0; t.a_b1 = d.b_b1; t.a_b2 = d.b_b2;
+  t.B = d.A; t.b_n = d.a_m; t.b_k = d.a_k; t.b_kb = d.a_kb; t.conjB = d.conjA;
+  t.b_b0 = d.a_b0; t.b_b1 = d.a_b1; t.b_b2 = d.a_b2;
+  t.c_m = d.c_n; t.c_n = d.c_m;
+  return t;
+}
+
+int8_t* zeroed_planes(DevBuf<int8_t>& b, size_t bytes, cudaStream_t st) {
+  if (bytes > b.n) {
+    b.ensure(bytes);
+    GG_CUDA(cudaMemsetAsync(b.p, 0, b.n, st));
+  }
+  return b.p;
+}
+
+// P0 of one k chunk (kn points from k0) and one spin in split precision.  The two operand builds
+// write the main contraction's int8 operand planes directly: no FP64 operand, no exponent scan
+// and no slicing pass.  Their scale per main row / column is a bound taken before the builds
+// (Cauchy-Schwarz, maximised over kk, a, b):
+//   |SA[kk][tt][Q'][a][b]| = |sum_p G^k(beta - tau)[a][p] V[kk][Q'][p][b]| <= max_a ||G row a|| max_b ||V[kk][Q'] column b||
+//   |SB[kk][tt][Q][a][b]|  = |sum_l conj(V[kk][Q][a][l]) G^{k+q}(tau)[b][l]| <= max_a ||V[kk][Q] row a|| max_b ||G row b||
+// which exceeds the row maximum by one to three bits (the exact-maximum scale of the slicing
+// pass would need a second pass over the operand).
+template <typename Main>
+void p0_split_block(gg_context* c, SplitGemm* split, const double2* Gf, const double2* G1, const double2* Vb,
+                    double2* P0q, int k0, int kn, int spa, const Plan& pl, double pref, bool first, cudaStream_t st,
+                    Main&& main) {
+  const auto& s = c->sh;
+  const int n = s.nao, N = s.NQ, T = s.nts, T2 = T / 2, S = c->slices, ns = gw_spins(c);
+  const long nn = (long)n * n, Nnn = (long)N * nn, NN = (long)N * N;
+  // the main contraction P0[t] (+)= pref/nk sum_kk sum_x SA[kk][tt][Q'][x] SB[kk][tt][Q][x]
+  auto main_desc = [&](int t0, int tn, int kb) {
+    ZgemmDesc d;
+    d.M = N; d.N = N; d.K = (int)nn; d.KB = kb;
+    d.C = P0q + (long)t0 * NN; d.c_m.lo = N; d.c_n.lo = 1;
+    d.nb0 = tn; d.c_b0 = NN;
+    d.alpha = make_double2(pref / s.nk, 0.0);
+    d.beta = first ? make_double2(0.0, 0.0) : make_double2(1.0, 0.0);
+    return d;
+  };
+  const SplitPlanes gmax = split_planes_for(main_desc(0, pl.tb, pl.kc), S);
+  int8_t* a8 = zeroed_planes(c->p0_a8, gmax.a_bytes, st);
+  int8_t* b8 = zeroed_planes(c->p0_b8, gmax.b_bytes, st);
+  int* ea = c->p0_ea.ensure((size_t)pl.tb * gmax.rows_a_pad);
+  int* eb = c->p0_eb.ensure((size_t)pl.tb * N);
+  double* v_col = c->p0_norms.ensure(2 * (size_t)pl.kc * N + 2 * (size_t)pl.kc * pl.tb);
+  double* v_row = v_col + (size_t)pl.kc * N;
+  double* g0 = v_row + (size_t)pl.kc * N;
+  double* g1 = g0 + (size_t)pl.kc * pl.tb;
+  launch_norm_max(Vb, kn, Nnn, N, nn, n, v_row, v_col, st);
+  c->launches += 1;
+  for (int t0 = 0; t0 < T2; t0 += pl.tb) {
+    const int tn = std::min(pl.tb, T2 - t0);
+    const ZgemmDesc dm = main_desc(t0, tn, kn);
+    const SplitPlanes g = split_planes_for(dm, S);
+    // G^k(tau_{T-1-t}) of (kk, tt) and G^{k+q}(tau_t) of (kk, tt): row-norm maxima
+    const double2* G0 = Gf + ((long)k0 * ns + spa) * T * nn + (long)(T - 1 - t0) * nn;
+    launch_norm_max(G0, kn, (long)ns * T * nn, tn, -nn, n, g0, nullptr, st);
+    launch_norm_max(G1 + (long)t0 * nn, kn, (long)T2 * nn, tn, nn, n, g1, nullptr, st);
+    launch_bound_exponents(g0, v_col, kn, tn, N, g.rows_a_pad, ea, st);
+    launch_bound_exponents(g1, v_row, kn, tn, N, N, eb, st);
+    c->launches += 4;
+    const int valid = (int)((2L * kn * nn) % 64);  // bytes of the last K block holding data
+    if (valid) {
+      launch_zero_kpad(a8, (long)tn * S, g.nkb, g.rows_a_pad, valid, st);
+      launch_zero_kpad(b8, (long)tn * S, g.nkb, g.rows_b_pad, valid, st);
+      c->launches += 2;
+    }
+    // A-build SA[kk][tt][Q'][a][b] = sum_p G^k(tau_{T-1-t})[a][p] V[kk][Q'][p][b], computed
+    // transposed: rows m = (Q', b), columns n = (tt, a), batch kk -> main A row Q' of batch tt,
+    // main K index kk nn + a n + b
+    {
+      ZgemmDesc d;
+      d.M = tn * n; d.N = N * n; d.K = n;
+      d.A = G0; d.a_m.split = n; d.a_m.hi = -nn; d.a_m.lo = n; d.a_k = 1;
+      d.B = Vb; d.b_k = n; d.b_n.split = n; d.b_n.hi = nn; d.b_n.lo = 1;
+      d.nb0 = kn;
+      d.a_b0 = (long)ns * T * nn; d.b_b0 = Nnn;
+      SplitEmit em;
+      em.on = 1; em.side = 0; em.div_m = n; em.div_n = n; em.batch_from_n = 1;
+      em.k_b = nn; em.k_m = 1; em.k_n = n;
+      em.nkb = g.nkb; em.rows = g.rows_a_pad; em.ex = ea; em.ex_ld = g.rows_a_pad; em.planes = a8;
+      c->launches += split_zgemm_emit(split, transposed(d), S, em, st);
+    }
+    // B-build SB[kk][tt][Q][a][b] = sum_l conj(V[kk][Q][a][l]) G^{k+q}(tau_t)[b][l], computed
+    // transposed: rows m = (tt, b), columns n = (Q, a) -> main B column Q of batch tt, same K index
+    {
+      ZgemmDesc d;
+      d.M = N * n; d.N = tn * n; d.K = n;
+      d.A = Vb; d.a_m.lo = n; d.a_k = 1; d.conjA = 1;
+      d.B = G1 + (long)t0 * nn; d.b_k = 1; d.b_n.split = n; d.b_n.hi = nn; d.b_n.lo = n;
+      d.nb0 = kn;
+      d.a_b0 = Nnn; d.b_b0 = (long)T2 * nn;
+      SplitEmit em;
+      em.on = 1; em.side = 1; em.div_m = n; em.div_n = n; em.batch_from_n = 0;
+      em.k_b = nn; em.k_m = 1; em.k_n = n;
+      em.nkb = g.nkb; em.rows = g.ncol_pad; em.ex = eb; em.ex_ld = N; em.planes = b8;
+      c->launches += split_zgemm_emit(split, transposed(d), S, em, st);
+    }
+    main(dm, a8, b8, ea, eb);
+  }
+}
+
+}  // namespace
+
 void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solver, int precision, cudaStream_t st) {
   if (!c->has_sym || !c->has_kpairs || !c->V || !c->has_ir || c->sh.nw_b <= 0)
     throw Error(GG_ERR_STATE, "gw: symmetry, k-pairs, integrals and IR transforms (nw_b > 0) must be set first");
@@ -281,7 +394,8 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
   c->Gtmp.ensure((size_t)nk * ns * T * nn);
   double2* Vb = c->Vbuf.ensure((size_t)pl.kc * Nnn);
   double2* G1 = c->G1buf.ensure((size_t)pl.kc * T2 * nn);
-  const size_t scr = std::max((size_t)pl.kc * pl.tb * Nnn, (size_t)T * std::max(Nnn, NN));
+  const size_t scr = std::max(precision == GG_PREC_SPLIT ? (size_t)0 : (size_t)pl.kc * pl.tb * Nnn,
+                              (size_t)T * std::max(Nnn, NN));
   double2* SA = c->scratchA.ensure(scr);
   double2* SB = c->scratchB.ensure(scr);
   double2* P0 = c->P0buf.ensure((size_t)pl.qc * T2 * NN);
@@ -313,14 +427,22 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
     c->kstat_seconds[i] = 0.0;
     c->kstat_flops[i] = 0.0;
   }
-  auto gemm_main = [&](ZgemmDesc d, int which, bool allow_split = true) {
+  struct Planes {
+    const int8_t* a8;
+    const int8_t* b8;
+    const int* ea;
+    const int* eb;
+  };
+  auto gemm_main = [&](ZgemmDesc d, int which, bool allow_split = true, const Planes* pr = nullptr) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c->profiling) {
       GG_CUDA(cudaEventCreate(&e0));
       GG_CUDA(cudaEventCreate(&e1));
       GG_CUDA(cudaEventRecord(e0, st));
     }
-    if (split && allow_split) {
+    if (split && pr) {
+      c->launches += split_zgemm_planes(split, d, c->slices, pr->a8, pr->b8, pr->ea, pr->eb, st);
+    } else if (split && allow_split) {
       d.work = gw_work;
       d.work_elems = (long)c->gemm_work.n;
       c->launches += split_zgemm(split, d, c->slices, st);
@@ -344,13 +466,7 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
   // C^T = B^T A^T (the same slices and int32 sums, so the same result).
   auto gemm_build = [&](ZgemmDesc d) {
     if (split) {
-      ZgemmDesc t = d;
-      t.M = d.N; t.N = d.M;
-      t.A = d.B; t.a_m = d.b_n; t.a_k = d.b_k; t.a_kb = d.b_kb; t.conjA = d.conjB;
-      t.a_b0 = d.b_b0; t.a_b1 = d.b_b1; t.a_b2 = d.b_b2;
-      t.B = d.A; t.b_n = d.a_m; t.b_k = d.a_k; t.b_kb = d.a_kb; t.conjB = d.conjA;
-      t.b_b0 = d.a_b0; t.b_b1 = d.a_b1; t.b_b2 = d.a_b2;
-      t.c_m = d.c_n; t.c_n = d.c_m;
+      ZgemmDesc t = transposed(d);
       t.work = gw_work;
       t.work_elems = (long)c->gemm_work.n;
       c->launches += split_zgemm(split, t, c->slices, st);
@@ -424,6 +540,15 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
           launch_gather_blocks(Gf, g1_idx.d.p + ((size_t)iq * ns + sp) * nk + k0, kn, (long)T2 * nn, (long)T * nn,
                                G1, st);
           ++c->launches;
+          if (split) {
+            p0_split_block(c, split, Gf, G1, Vb, P0 + (long)qi * T2 * NN, k0, kn, spin_a(sp), pl, pref,
+                           (sp == 0 && k0 == 0), st,
+                           [&](const ZgemmDesc& d, const int8_t* a8, const int8_t* b8, const int* ea, const int* eb) {
+                             const Planes pr{a8, b8, ea, eb};
+                             gemm_main(d, 0, true, &pr);
+                           });
+            continue;
+          }
           for (int t0 = 0; t0 < T2; t0 += pl.tb) {
             const int tn = std::min(pl.tb, T2 - t0);
             // A-build: SA[kk][tt][Q'][a][b] = sum_p G^k(tau_{T-1-t})[a][p] V[kk][Q'][p][b].

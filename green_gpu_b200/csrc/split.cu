@@ -181,6 +181,9 @@ __device__ __forceinline__ double pow2i(int e) {
   return __longlong_as_double((long long)(e + 1023) << 52);
 }
 
+// 2^e for e in the normal range (exact)
+__device__ __forceinline__ double scale_pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+
 // drain `NC` int32 columns (a multiple of 8, at most 32) starting at taddr into acc * scale
 template <int NC>
 __device__ __forceinline__ void drain_cols(uint32_t taddr, double* acc, double scale) {
@@ -196,6 +199,47 @@ __device__ __forceinline__ void drain_cols(uint32_t taddr, double* acc, double s
     // exact int32 -> double: the bits (0x43380000, r + 2^31) encode 2^52 + 2^51 + r + 2^31
     const double x = __hiloint2double(0x43380000, r[i] ^ (int)0x80000000) - 6755401588539392.0;
     acc[i] = fma(x, scale, acc[i]);
+  }
+}
+
+// Write x (a value of the target operand, |x| < 2^e) as S int8 slices at K index k of target
+// row (A planes) or complex column (B planes) `tr` of target batch `tb`.  X = rint(x 2^(7S-1-e))
+// (|X| <= 2^(7S-1)) is split into base-128 digits, the lower S - 1 balanced in [-63, 64] and the
+// top one the remaining quotient (|d_1| <= 64), by exact integer arithmetic, so that
+// x = 2^(e+1) sum_s d_s 2^-7s up to the rounding of X (|error| <= 2^(e-7S)).
+template <int S>
+__device__ __forceinline__ void emit_slices(double2 v, int e, const SplitEmit& em, long tb, int tr, long k) {
+  const double f = scale_pow2(7 * S - 1 - e);
+  long long xr = __double2ll_rn(v.x * f), xi = __double2ll_rn(v.y * f);
+  int8_t dr[S], di[S];
+#pragma unroll
+  for (int s = S - 1; s >= 1; --s) {
+    int r = (int)(xr & 127), i = (int)(xi & 127);
+    r -= (r > 64) ? 128 : 0;
+    i -= (i > 64) ? 128 : 0;
+    dr[s] = (int8_t)r;
+    di[s] = (int8_t)i;
+    xr = (xr - r) >> 7;
+    xi = (xi - i) >> 7;
+  }
+  dr[0] = (int8_t)xr;
+  di[0] = (int8_t)xi;
+  const long kb = k >> 5;
+  const int off = 2 * (int)(k & 31);
+  if (em.side == 0) {
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      int8_t* o = em.planes + ((((tb * S + s) * em.nkb + kb) * em.rows + tr) << 6) + off;
+      *(char2*)o = make_char2(dr[s], di[s]);
+    }
+  } else {
+    // B' rows 2c: (re, -im); 2c + 1: (im, re)
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      int8_t* o = em.planes + ((((tb * S + s) * em.nkb + kb) * (2L * em.rows) + 2L * tr) << 6) + off;
+      *(char2*)o = make_char2(dr[s], (int8_t)(-di[s]));
+      *(char2*)(o + 64) = make_char2(di[s], dr[s]);
+    }
   }
 }
 
@@ -222,6 +266,8 @@ struct I8Args {
   int nbuf;  // accumulator sets in TMEM (1 or 2)
   int a_shared, b_shared;  // operand identical for every batch: sliced once, planes / exponents of batch 0
   int* err;
+  SplitEmit em;            // em.on: the epilogue writes the product as int8 slices of another split
+                           // GEMM's operand instead of writing C
   long long wait_cycles;   // limit of every barrier wait (WAIT_CYCLES; shorter in the time-out test)
   int skip_arrive;         // time-out test: CTA 0's first epilogue warp never releases the first
                            // drained accumulator, so the MMA warp's wait for it must run out
@@ -499,6 +545,30 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       const double sa = pow2i(ea);  // row factor; x = 2 sum d_s 2^-7s per operand gives the + 2
       double2* crow = p.C + b0 * p.c_b0 + b1 * p.c_b1 + b2 * p.c_b2 + (mok ? p.c_m(m) : 0);
       double2* wrow = p.work + (w.split * p.batch + w.batch) * (long)p.N * p.M + m;
+      if (p.em.on) {
+        // the product as slices of the target operand: (m, n, batch) -> target (batch, row or
+        // column, K index); the target's exponent comes from a bound computed beforehand
+        const SplitEmit& em = p.em;
+        const int mq = m / em.div_m, mr = m - mq * em.div_m;
+        int eq = nbase / em.div_n, er = nbase - eq * em.div_n;
+        const long kbase = w.batch * em.k_b + (long)mr * em.k_m;
+#pragma unroll
+        for (int c = 0; c < HC / 2; ++c) {
+          const int eb = __shfl_sync(0xffffffffu, eb_lane, c);
+          if (mok && nbase + c < p.N) {
+            const double sb = pow2i(eb + 2);
+            const double2 v = make_double2(acc[2 * c] * sa * sb, acc[2 * c + 1] * sa * sb);
+            const long tb = em.batch_from_n ? eq : mq;
+            const int tr = em.batch_from_n ? mq : eq;
+            emit_slices<S>(v, em.ex[tb * em.ex_ld + tr], em, tb, tr, kbase + (long)er * em.k_n);
+          }
+          if (++er == em.div_n) {
+            er = 0;
+            ++eq;
+          }
+        }
+        continue;
+      }
       // column offset c_n(n) stepped through the tile: (nq, nr) = divmod(n, split)
       const int csp = p.c_n.split > 0 ? p.c_n.split : 1 << 30;
       int nq = nbase / csp, nr = nbase - nq * csp;
@@ -826,75 +896,61 @@ void split_buffers(const SplitGemm* e, std::vector<const void*>& out) {
   out.insert(out.end(), {e->a8.p, e->b8.p, e->ea.p, e->eb.p, e->err.p, e->work.p});
 }
 
-int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
+namespace {
+
+// tile geometry of a split GEMM with S slices
+struct Geometry {
+  int BN, nbuf, rows_a_pad, rows_b_pad, ncol_pad, nkb, kcb;
+  long batch, Ktot, kp;
+};
+
+Geometry geometry(const ZgemmDesc& d, int S) {
   if (S < 2 || S > 8) throw Error(GG_ERR_ARG, "split: slices must be in [2, 8]");
-  if (d.M <= 0 || d.N <= 0) return 0;
+  Geometry g;
   // nbuf accumulator sets of S diagonals x BN columns must fit the 512 TMEM columns;
   // BN <= 128 keeps the FP64 drain registers (BN / 2 per thread) in budget
-  const int nbuf = S <= 2 ? 2 : 1;
-  const int BN = S <= 4 ? 128 : S == 5 ? 96 : S == 6 ? 80 : 64;
-  const long batch = (long)d.nb0 * d.nb1 * d.nb2;
-  const long Ktot = (long)d.KB * d.K;
-  if (2 * Ktot + KB >= (1L << 31) || (long)d.M >= (1L << 31) || (long)d.N >= (1L << 30))
+  g.nbuf = S <= 2 ? 2 : 1;
+  g.BN = S <= 4 ? 128 : S == 5 ? 96 : S == 6 ? 80 : 64;
+  g.batch = (long)d.nb0 * d.nb1 * d.nb2;
+  g.Ktot = (long)d.KB * d.K;
+  if (2 * g.Ktot + KB >= (1L << 31) || (long)d.M >= (1L << 31) || (long)d.N >= (1L << 30))
     throw Error(GG_ERR_ARG, "split: operand dimensions too large for one launch");
-  const long kp = ((2 * Ktot + KB - 1) / KB) * KB;
-  const int rows_a_pad = ((d.M + BM - 1) / BM) * BM;
-  const int np = 2 * d.N;
-  const int rows_b_pad = ((np + BN - 1) / BN) * BN;  // B' rows (2 per complex column), whole tiles
-  const int ncol_pad = rows_b_pad / 2;                // complex columns incl. padding
+  g.kp = ((2 * g.Ktot + KB - 1) / KB) * KB;
+  g.rows_a_pad = ((d.M + BM - 1) / BM) * BM;
+  g.rows_b_pad = ((2 * d.N + g.BN - 1) / g.BN) * g.BN;  // B' rows (2 per complex column), whole tiles
+  g.ncol_pad = g.rows_b_pad / 2;                        // complex columns incl. padding
   // exact int32 chunk: S * Kchunk * 64^2 < 2^31 (slices are rounded, |d| <= 64)
   const long kchunk = std::max<long>(KB, ((2147483647L / (4096L * S)) / KB) * KB);
-  const int kcb = (int)(kchunk / KB);
-  const int nkb = (int)(kp / KB);
+  g.kcb = (int)(kchunk / KB);
+  g.nkb = (int)(g.kp / KB);
+  return g;
+}
 
-  // an operand with zero batch strides is the same matrix for every batch: slice it once
-  const bool a_shared = batch > 1 && d.a_b0 == 0 && d.a_b1 == 0 && d.a_b2 == 0;
-  const bool b_shared = batch > 1 && d.b_b0 == 0 && d.b_b1 == 0 && d.b_b2 == 0;
-  const long batch_a = a_shared ? 1 : batch, batch_b = b_shared ? 1 : batch;
-  int8_t* a8 = e->a8.ensure((size_t)batch_a * S * rows_a_pad * kp);
-  int8_t* b8 = e->b8.ensure((size_t)batch_b * S * rows_b_pad * kp);
-  int* ea = e->ea.ensure((size_t)batch_a * rows_a_pad);
-  int* eb = e->eb.ensure((size_t)batch_b * d.N);
+// the persistent INT8 GEMM on operand planes (a8 / b8 of batch_a / batch_b batches)
+int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const int8_t* a8, const int8_t* b8,
+               const int* ea, const int* eb, bool a_shared, bool b_shared, const SplitEmit* em, cudaStream_t st) {
   int* err = e->err.p;
   if (!err) {
     err = e->err.ensure(1);
     GG_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
   }
-
-  OpView va{d.A, d.a_m, d.a_kb, d.a_k, d.KB, d.K, d.M, d.nb0, d.nb1, d.a_b0, d.a_b1, d.a_b2, d.conjA};
-  OpView vb{d.B, d.b_n, d.b_kb, d.b_k, d.KB, d.K, d.N, d.nb0, d.nb1, d.b_b0, d.b_b1, d.b_b2, d.conjB};
-  int launches = 0;
-  {
-    auto exponents = [&](const OpView& v, int rows_pad, int* out, long nb) {
-      const bool rcontig = v.rmap.lo == 1 && v.ks != 1;
-      const long n = nb * rows_pad;
-      if (rcontig)
-        row_exponent_rc_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(v, rows_pad, out, nb);
-      else
-        row_exponent_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(v, rows_pad, out, nb);
-      GG_CHECK_LAUNCH();
-    };
-    exponents(va, rows_a_pad, ea, batch_a);
-    exponents(vb, d.N, eb, batch_b);
-    launch_slices(S, va, vb, rows_a_pad, ncol_pad, nkb, ea, eb, a8, b8, batch_a, batch_b, st);
-    launches += 4;
-  }
-  const CUtensorMap ta = make_map(a8, rows_a_pad, batch_a * S * nkb, BM);
-  const CUtensorMap tb = make_map(b8, rows_b_pad, batch_b * S * nkb, BN);
+  const long batch_a = a_shared ? 1 : g.batch, batch_b = b_shared ? 1 : g.batch;
+  const CUtensorMap ta = make_map(a8, g.rows_a_pad, batch_a * S * g.nkb, BM);
+  const CUtensorMap tb = make_map(b8, g.rows_b_pad, batch_b * S * g.nkb, g.BN);
 
   I8Args a{};
   a.S = S;
-  a.rows_a_pad = rows_a_pad;
-  a.rows_b_pad = rows_b_pad;
-  a.nkb = nkb;
-  a.kcb = kcb;
+  a.rows_a_pad = g.rows_a_pad;
+  a.rows_b_pad = g.rows_b_pad;
+  a.nkb = g.nkb;
+  a.kcb = g.kcb;
   a.M = d.M;
   a.N = d.N;
-  a.tiles_m = rows_a_pad / BM;
-  a.tiles_n = rows_b_pad / BN;
+  a.tiles_m = g.rows_a_pad / BM;
+  a.tiles_n = g.rows_b_pad / g.BN;
   a.nb0 = d.nb0;
   a.nb1 = d.nb1;
-  a.batch = batch;
+  a.batch = g.batch;
   a.ea = ea;
   a.eb = eb;
   a.C = d.C;
@@ -906,6 +962,7 @@ int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
   a.alpha = d.alpha;
   a.beta = d.beta;
   a.err = err;
+  if (em) a.em = *em;
   a.wait_cycles = WAIT_CYCLES;
   a.skip_arrive = 0;
   if (e->timeout_test) {
@@ -915,20 +972,21 @@ int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
     a.skip_arrive = 1;
     e->timeout_test = false;
   }
-  a.nbuf = nbuf;
+  a.nbuf = g.nbuf;
   a.a_shared = a_shared ? 1 : 0;
   a.b_shared = b_shared ? 1 : 0;
   a.tmem_cols = 32;
-  while (a.tmem_cols < nbuf * S * BN) a.tmem_cols *= 2;
-  const size_t stage_bytes = (size_t)S * (BM + BN) * KB;
+  while (a.tmem_cols < g.nbuf * S * g.BN) a.tmem_cols *= 2;
+  const size_t stage_bytes = (size_t)S * (BM + g.BN) * KB;
   a.stages = (int)std::min<size_t>(4, (220 * 1024 - 2048) / stage_bytes);
   if (a.stages < 2) throw Error(GG_ERR_ARG, "split: stage does not fit shared memory");
   const size_t smem = a.stages * stage_bytes + 1024 + 512;  // + alignment + barriers and TMEM slot
-  const long base = (long)a.tiles_m * a.tiles_n * batch;
-  // split-K so that the units fill whole waves of persistent CTAs (each split keeps >= 8 K blocks)
+  const long base = (long)a.tiles_m * a.tiles_n * g.batch;
+  // split-K so that the units fill whole waves of persistent CTAs (each split keeps >= 8 K
+  // blocks); an emitting epilogue needs whole reductions (no split-K)
   int splits = 1;
-  {
-    const int smax = (int)std::max<long>(1, std::min<long>(nkb / 8, 64));
+  if (!a.em.on) {
+    const int smax = (int)std::max<long>(1, std::min<long>(g.nkb / 8, 64));
     double best = 0.0;
     for (int sp = 1; sp <= smax; ++sp) {
       const long units = base * sp;
@@ -942,17 +1000,17 @@ int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
       if (units >= 4L * sms()) break;
     }
   }
-  const long need = (long)d.M * d.N * batch;
+  const long need = (long)d.M * d.N * g.batch;
   if (splits > 1) {
     e->work.ensure((size_t)splits * need);
   }
   a.splits = splits;
   a.work = e->work.p;
   a.units = base * splits;
-  if (a.units >= (1L << 31) || (long)splits * nkb >= (1L << 31))
+  if (a.units >= (1L << 31) || (long)splits * g.nkb >= (1L << 31))
     throw Error(GG_ERR_ARG, "split: too many work units for one launch");
   const long grid = std::min<long>(a.units, sms());
-  switch (S) {  // BN as chosen above for each slice count
+  switch (S) {  // BN as chosen in geometry() for each slice count
     case 2: launch_i8<2, 128>(ta, tb, a, grid, smem, st); break;
     case 3: launch_i8<3, 128>(ta, tb, a, grid, smem, st); break;
     case 4: launch_i8<4, 128>(ta, tb, a, grid, smem, st); break;
@@ -961,16 +1019,77 @@ int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) {
     case 7: launch_i8<7, 64>(ta, tb, a, grid, smem, st); break;
     default: launch_i8<8, 64>(ta, tb, a, grid, smem, st); break;
   }
-  ++launches;
+  int launches = 1;
   if (splits > 1) {
     const long total = need;
     const long nblk = std::min<long>((total + 255) / 256, 65535L * 8);
-    split_reduce_kernel<<<(unsigned)nblk, 256, 0, st>>>(e->work.p, splits, batch, d.M, d.N, d.C, d.c_m, d.c_n, d.nb0,
-                                                       d.nb1, d.c_b0, d.c_b1, d.c_b2, d.alpha, d.beta);
+    split_reduce_kernel<<<(unsigned)nblk, 256, 0, st>>>(e->work.p, splits, g.batch, d.M, d.N, d.C, d.c_m, d.c_n,
+                                                       d.nb0, d.nb1, d.c_b0, d.c_b1, d.c_b2, d.alpha, d.beta);
     GG_CHECK_LAUNCH();
     ++launches;
   }
   return launches;
+}
+
+// exponents and slices of both operands into the engine's planes, then the GEMM
+int sliced_gemm(SplitGemm* e, const ZgemmDesc& d, int S, const SplitEmit* em, cudaStream_t st) {
+  if (d.M <= 0 || d.N <= 0) return 0;
+  const Geometry g = geometry(d, S);
+  // an operand with zero batch strides is the same matrix for every batch: slice it once
+  const bool a_shared = g.batch > 1 && d.a_b0 == 0 && d.a_b1 == 0 && d.a_b2 == 0;
+  const bool b_shared = g.batch > 1 && d.b_b0 == 0 && d.b_b1 == 0 && d.b_b2 == 0;
+  const long batch_a = a_shared ? 1 : g.batch, batch_b = b_shared ? 1 : g.batch;
+  int8_t* a8 = e->a8.ensure((size_t)batch_a * S * g.rows_a_pad * g.kp);
+  int8_t* b8 = e->b8.ensure((size_t)batch_b * S * g.rows_b_pad * g.kp);
+  int* ea = e->ea.ensure((size_t)batch_a * g.rows_a_pad);
+  int* eb = e->eb.ensure((size_t)batch_b * d.N);
+  OpView va{d.A, d.a_m, d.a_kb, d.a_k, d.KB, d.K, d.M, d.nb0, d.nb1, d.a_b0, d.a_b1, d.a_b2, d.conjA};
+  OpView vb{d.B, d.b_n, d.b_kb, d.b_k, d.KB, d.K, d.N, d.nb0, d.nb1, d.b_b0, d.b_b1, d.b_b2, d.conjB};
+  auto exponents = [&](const OpView& v, int rows_pad, int* out, long nb) {
+    const bool rcontig = v.rmap.lo == 1 && v.ks != 1;
+    const long n = nb * rows_pad;
+    if (rcontig)
+      row_exponent_rc_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(v, rows_pad, out, nb);
+    else
+      row_exponent_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(v, rows_pad, out, nb);
+    GG_CHECK_LAUNCH();
+  };
+  exponents(va, g.rows_a_pad, ea, batch_a);
+  exponents(vb, d.N, eb, batch_b);
+  launch_slices(S, va, vb, g.rows_a_pad, g.ncol_pad, g.nkb, ea, eb, a8, b8, batch_a, batch_b, st);
+  return 4 + run_planes(e, d, S, g, a8, b8, ea, eb, a_shared, b_shared, em, st);
+}
+
+}  // namespace
+
+SplitPlanes split_planes_for(const ZgemmDesc& d, int S) {
+  const Geometry g = geometry(d, S);
+  SplitPlanes p;
+  p.rows_a_pad = g.rows_a_pad;
+  p.rows_b_pad = g.rows_b_pad;
+  p.ncol_pad = g.ncol_pad;
+  p.nkb = g.nkb;
+  p.batch = g.batch;
+  p.a_bytes = (size_t)g.batch * S * g.rows_a_pad * g.kp;
+  p.b_bytes = (size_t)g.batch * S * g.rows_b_pad * g.kp;
+  return p;
+}
+
+int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) { return sliced_gemm(e, d, S, nullptr, st); }
+
+int split_zgemm_emit(SplitGemm* e, const ZgemmDesc& d, int S, const SplitEmit& em, cudaStream_t st) {
+  if (!em.on || !em.planes || !em.ex || em.div_m < 1 || em.div_n < 1 || em.nkb < 1 || em.rows < 1)
+    throw Error(GG_ERR_ARG, "split emit: incomplete target description");
+  if (d.alpha.x != 1.0 || d.alpha.y != 0.0 || d.beta.x != 0.0 || d.beta.y != 0.0)
+    throw Error(GG_ERR_ARG, "split emit: alpha must be 1 and beta 0");
+  return sliced_gemm(e, d, S, &em, st);
+}
+
+int split_zgemm_planes(SplitGemm* e, const ZgemmDesc& d, int S, const int8_t* a8, const int8_t* b8, const int* ea,
+                       const int* eb, cudaStream_t st) {
+  if (d.M <= 0 || d.N <= 0) return 0;
+  const Geometry g = geometry(d, S);
+  return run_planes(e, d, S, g, a8, b8, ea, eb, false, false, nullptr, st);
 }
 
 void split_check(SplitGemm* e, cudaStream_t st) {

@@ -30,7 +30,8 @@ def test_split_wait_runs_out_and_the_context_recovers():
     assert "timed out" in str(e.value)
     # the same context and engine work again
     out = ctx.zgemm(A, B, precision=native.PREC_SPLIT)
-    assert np.abs(out - ref).max() < 1e-9 * np.abs(ref).max()
+    # the engine's error bound at 5 slices: 2^(-7 S + 4) sqrt(K) of the largest element
+    assert np.abs(out - ref).max() < 2.0 ** (-7 * 5 + 4) * np.sqrt(K) * np.abs(ref).max()
     ctx.close()
     s = synth.make_system(mesh=(2, 2, 1), nao=8, NQ=24, ns=1, beta=10.0, lam=100.0, nts=24, nw_b=21, seed=9,
                           symmetry="none")
