@@ -910,7 +910,21 @@ Geometry geometry(const ZgemmDesc& d, int S) {
   // nbuf accumulator sets of S diagonals x BN columns must fit the 512 TMEM columns;
   // BN <= 128 keeps the FP64 drain registers (BN / 2 per thread) in budget
   g.nbuf = S <= 2 ? 2 : 1;
+  // tile width: the widest one whose accumulators fit TMEM, or a narrower one that pads the
+  // 2N rows of B' less (2N = 800: 80 divides it, 96 pads it to 864)
   g.BN = S <= 4 ? 128 : S == 5 ? 96 : S == 6 ? 80 : 64;
+  if (S == 5 || S == 6) {
+    const int cands[3] = {96, 80, 64};
+    long best = -1;
+    for (int bn : cands) {
+      if (S == 6 && bn == 96) continue;
+      const long pad = ((2L * d.N + bn - 1) / bn) * bn;
+      if (best < 0 || pad < best) {
+        best = pad;
+        g.BN = bn;
+      }
+    }
+  }
   g.batch = (long)d.nb0 * d.nb1 * d.nb2;
   g.Ktot = (long)d.KB * d.K;
   if (2 * g.Ktot + KB >= (1L << 31) || (long)d.M >= (1L << 31) || (long)d.N >= (1L << 30))
@@ -1010,14 +1024,18 @@ int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const
   if (a.units >= (1L << 31) || (long)splits * g.nkb >= (1L << 31))
     throw Error(GG_ERR_ARG, "split: too many work units for one launch");
   const long grid = std::min<long>(a.units, sms());
-  switch (S) {  // BN as chosen in geometry() for each slice count
-    case 2: launch_i8<2, 128>(ta, tb, a, grid, smem, st); break;
-    case 3: launch_i8<3, 128>(ta, tb, a, grid, smem, st); break;
-    case 4: launch_i8<4, 128>(ta, tb, a, grid, smem, st); break;
-    case 5: launch_i8<5, 96>(ta, tb, a, grid, smem, st); break;
-    case 6: launch_i8<6, 80>(ta, tb, a, grid, smem, st); break;
-    case 7: launch_i8<7, 64>(ta, tb, a, grid, smem, st); break;
-    default: launch_i8<8, 64>(ta, tb, a, grid, smem, st); break;
+  switch (S * 1000 + g.BN) {  // the (S, BN) pairs geometry() chooses
+    case 2128: launch_i8<2, 128>(ta, tb, a, grid, smem, st); break;
+    case 3128: launch_i8<3, 128>(ta, tb, a, grid, smem, st); break;
+    case 4128: launch_i8<4, 128>(ta, tb, a, grid, smem, st); break;
+    case 5096: launch_i8<5, 96>(ta, tb, a, grid, smem, st); break;
+    case 5080: launch_i8<5, 80>(ta, tb, a, grid, smem, st); break;
+    case 5064: launch_i8<5, 64>(ta, tb, a, grid, smem, st); break;
+    case 6080: launch_i8<6, 80>(ta, tb, a, grid, smem, st); break;
+    case 6064: launch_i8<6, 64>(ta, tb, a, grid, smem, st); break;
+    case 7064: launch_i8<7, 64>(ta, tb, a, grid, smem, st); break;
+    case 8064: launch_i8<8, 64>(ta, tb, a, grid, smem, st); break;
+    default: throw Error(GG_ERR_INTERNAL, "split: no kernel for this slice count and tile width");
   }
   int launches = 1;
   if (splits > 1) {
