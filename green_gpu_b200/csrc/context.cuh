@@ -97,12 +97,9 @@ struct gg_context {
   gg::DevBuf<double2> G_in, Sigma_out, Gf, Gtmp, Vbuf, G1buf, scratchA, scratchB, P0buf, Pw, Afac, Wt, Wrot,
       gemm_work, hf_D, hf_F, hf_c, hf_J;
   gg::DevBuf<int> info, piv, idx_i;
-  // split precision: int8 planes of the P0 main contraction's operands, written directly by the
-  // operand builds (zeroed when allocated, so their padding stays zero), their exponent bounds,
-  // and the row / column norm maxima the bounds come from
-  gg::DevBuf<int8_t> p0_a8, p0_b8;
+  // split precision: exponents of the P0 main contraction's operand rows / columns, recorded
+  // by the operand builds' epilogues
   gg::DevBuf<int> p0_ea, p0_eb;
-  gg::DevBuf<double> p0_norms;
   gg::DevBuf<int64_t> pos_d;
   gg::DevBuf<int> op_d;
 

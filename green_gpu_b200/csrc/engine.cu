@@ -189,7 +189,7 @@ Plan plan_gw(gg_context* c, int slices) {
     b += 2 * (size_t)s.nk * nspin * s.nts * nn;       // Gf + Gtmp
     b += (size_t)q.kc * Nnn;                           // Vbuf
     b += (size_t)q.kc * T2 * nn;                       // G1buf
-    size_t p0s = slices > 0 ? 0 : (size_t)q.kc * q.tb * Nnn;  // FP64 A / B build buffers (each)
+    size_t p0s = (size_t)q.kc * q.tb * Nnn;            // A / B build buffers (each)
     size_t sgs = (size_t)s.nts * std::max(Nnn, NN);    // Sigma X / Z, W rotation (each)
     b += 2 * std::max(p0s, sgs);
     b += (size_t)q.qc * T2 * NN;                       // P0
@@ -260,99 +260,66 @@ ZgemmDesc transposed(const ZgemmDesc& d) {
   return t;
 }
 
-int8_t* zeroed_planes(DevBuf<int8_t>& b, size_t bytes, cudaStream_t st) {
-  if (bytes > b.n) {
-    b.ensure(bytes);
-    GG_CUDA(cudaMemsetAsync(b.p, 0, b.n, st));
-  }
-  return b.p;
-}
-
-// P0 of one k chunk (kn points from k0) and one spin in split precision.  The two operand builds
-// write the main contraction's int8 operand planes directly: no FP64 operand, no exponent scan
-// and no slicing pass.  Their scale per main row / column is a bound taken before the builds
-// (Cauchy-Schwarz, maximised over kk, a, b):
-//   |SA[kk][tt][Q'][a][b]| = |sum_p G^k(beta - tau)[a][p] V[kk][Q'][p][b]| <= max_a ||G row a|| max_b ||V[kk][Q'] column b||
-//   |SB[kk][tt][Q][a][b]|  = |sum_l conj(V[kk][Q][a][l]) G^{k+q}(tau)[b][l]| <= max_a ||V[kk][Q] row a|| max_b ||G row b||
-// which exceeds the row maximum by one to three bits (the exact-maximum scale of the slicing
-// pass would need a second pass over the operand).
+// P0 of one k chunk (kn points from k0) and one spin in split precision.  The operand builds
+// (INT8 engine, FP64 output SA / SB as in the FP64 path) also record the exact maximum of every
+// row of SA and every column of SB that the main contraction slices with (a segmented warp
+// reduction and one atomicMax per row segment in their epilogue), so the two exponent scans over
+// SA and SB - a full read of both - are not needed; the slicing pass uses those exponents.
 template <typename Main>
 void p0_split_block(gg_context* c, SplitGemm* split, const double2* Gf, const double2* G1, const double2* Vb,
-                    double2* P0q, int k0, int kn, int spa, const Plan& pl, double pref, bool first, cudaStream_t st,
-                    Main&& main) {
+                    double2* SA, double2* SB, double2* P0q, int k0, int kn, int spa, const Plan& pl, double pref,
+                    bool first, cudaStream_t st, Main&& main) {
   const auto& s = c->sh;
   const int n = s.nao, N = s.NQ, T = s.nts, T2 = T / 2, S = c->slices, ns = gw_spins(c);
   const long nn = (long)n * n, Nnn = (long)N * nn, NN = (long)N * N;
-  // the main contraction P0[t] (+)= pref/nk sum_kk sum_x SA[kk][tt][Q'][x] SB[kk][tt][Q][x]
-  auto main_desc = [&](int t0, int tn, int kb) {
-    ZgemmDesc d;
-    d.M = N; d.N = N; d.K = (int)nn; d.KB = kb;
-    d.C = P0q + (long)t0 * NN; d.c_m.lo = N; d.c_n.lo = 1;
-    d.nb0 = tn; d.c_b0 = NN;
-    d.alpha = make_double2(pref / s.nk, 0.0);
-    d.beta = first ? make_double2(0.0, 0.0) : make_double2(1.0, 0.0);
-    return d;
-  };
-  const SplitPlanes gmax = split_planes_for(main_desc(0, pl.tb, pl.kc), S);
-  int8_t* a8 = zeroed_planes(c->p0_a8, gmax.a_bytes, st);
-  int8_t* b8 = zeroed_planes(c->p0_b8, gmax.b_bytes, st);
-  int* ea = c->p0_ea.ensure((size_t)pl.tb * gmax.rows_a_pad);
-  int* eb = c->p0_eb.ensure((size_t)pl.tb * N);
-  double* v_col = c->p0_norms.ensure(2 * (size_t)pl.kc * N + 2 * (size_t)pl.kc * pl.tb);
-  double* v_row = v_col + (size_t)pl.kc * N;
-  double* g0 = v_row + (size_t)pl.kc * N;
-  double* g1 = g0 + (size_t)pl.kc * pl.tb;
-  launch_norm_max(Vb, kn, Nnn, N, nn, n, v_row, v_col, st);
-  c->launches += 1;
   for (int t0 = 0; t0 < T2; t0 += pl.tb) {
     const int tn = std::min(pl.tb, T2 - t0);
-    const ZgemmDesc dm = main_desc(t0, tn, kn);
+    // P0[t] (+)= pref/nk sum_kk sum_x SA[kk][tt][Q'][x] SB[kk][tt][Q][x]
+    ZgemmDesc dm;
+    dm.M = N; dm.N = N; dm.K = (int)nn; dm.KB = kn;
+    dm.A = SA; dm.a_m.lo = nn; dm.a_k = 1; dm.a_kb = (long)tn * Nnn;
+    dm.B = SB; dm.b_k = 1; dm.b_n.lo = nn; dm.b_kb = (long)tn * Nnn;
+    dm.C = P0q + (long)t0 * NN; dm.c_m.lo = N; dm.c_n.lo = 1;
+    dm.nb0 = tn; dm.a_b0 = Nnn; dm.b_b0 = Nnn; dm.c_b0 = NN;
+    dm.alpha = make_double2(pref / s.nk, 0.0);
+    dm.beta = first ? make_double2(0.0, 0.0) : make_double2(1.0, 0.0);
     const SplitPlanes g = split_planes_for(dm, S);
-    // G^k(tau_{T-1-t}) of (kk, tt) and G^{k+q}(tau_t) of (kk, tt): row-norm maxima
-    const double2* G0 = Gf + ((long)k0 * ns + spa) * T * nn + (long)(T - 1 - t0) * nn;
-    launch_norm_max(G0, kn, (long)ns * T * nn, tn, -nn, n, g0, nullptr, st);
-    launch_norm_max(G1 + (long)t0 * nn, kn, (long)T2 * nn, tn, nn, n, g1, nullptr, st);
-    launch_bound_exponents(g0, v_col, kn, tn, N, g.rows_a_pad, ea, st);
-    launch_bound_exponents(g1, v_row, kn, tn, N, N, eb, st);
-    c->launches += 4;
-    const int valid = (int)((2L * kn * nn) % 64);  // bytes of the last K block holding data
-    if (valid) {
-      launch_zero_kpad(a8, (long)tn * S, g.nkb, g.rows_a_pad, valid, st);
-      launch_zero_kpad(b8, (long)tn * S, g.nkb, g.rows_b_pad, valid, st);
-      c->launches += 2;
-    }
+    int* ea = c->p0_ea.ensure((size_t)pl.tb * g.rows_a_pad);
+    int* eb = c->p0_eb.ensure((size_t)pl.tb * N);
+    // every exponent starts below any value's (bytes 0x80: -2139062144)
+    GG_CUDA(cudaMemsetAsync(ea, 0x80, sizeof(int) * (size_t)tn * g.rows_a_pad, st));
+    GG_CUDA(cudaMemsetAsync(eb, 0x80, sizeof(int) * (size_t)tn * N, st));
     // A-build SA[kk][tt][Q'][a][b] = sum_p G^k(tau_{T-1-t})[a][p] V[kk][Q'][p][b], computed
-    // transposed: rows m = (Q', b), columns n = (tt, a), batch kk -> main A row Q' of batch tt,
-    // main K index kk nn + a n + b
+    // transposed: rows m = (Q', b), columns n = (tt, a); main A row Q' of batch tt
     {
       ZgemmDesc d;
       d.M = tn * n; d.N = N * n; d.K = n;
-      d.A = G0; d.a_m.split = n; d.a_m.hi = -nn; d.a_m.lo = n; d.a_k = 1;
+      d.A = Gf + ((long)k0 * ns + spa) * T * nn + (long)(T - 1 - t0) * nn;
+      d.a_m.split = n; d.a_m.hi = -nn; d.a_m.lo = n; d.a_k = 1;
       d.B = Vb; d.b_k = n; d.b_n.split = n; d.b_n.hi = nn; d.b_n.lo = 1;
+      d.C = SA; d.c_m.split = n; d.c_m.hi = Nnn; d.c_m.lo = n;
+      d.c_n.split = n; d.c_n.hi = nn; d.c_n.lo = 1;
       d.nb0 = kn;
-      d.a_b0 = (long)ns * T * nn; d.b_b0 = Nnn;
-      SplitEmit em;
-      em.on = 1; em.side = 0; em.div_m = n; em.div_n = n; em.batch_from_n = 1;
-      em.k_b = nn; em.k_m = 1; em.k_n = n;
-      em.nkb = g.nkb; em.rows = g.rows_a_pad; em.ex = ea; em.ex_ld = g.rows_a_pad; em.planes = a8;
-      c->launches += split_zgemm_emit(split, transposed(d), S, em, st);
+      d.a_b0 = (long)ns * T * nn; d.b_b0 = Nnn; d.c_b0 = (long)tn * Nnn;
+      SplitRowMax mx;
+      mx.on = 1; mx.div_m = n; mx.div_n = n; mx.batch_from_n = 1; mx.ld = g.rows_a_pad; mx.ex = ea;
+      c->launches += split_zgemm_rowmax(split, transposed(d), S, mx, st);
     }
     // B-build SB[kk][tt][Q][a][b] = sum_l conj(V[kk][Q][a][l]) G^{k+q}(tau_t)[b][l], computed
-    // transposed: rows m = (tt, b), columns n = (Q, a) -> main B column Q of batch tt, same K index
+    // transposed: rows m = (tt, b), columns n = (Q, a); main B column Q of batch tt
     {
       ZgemmDesc d;
       d.M = N * n; d.N = tn * n; d.K = n;
       d.A = Vb; d.a_m.lo = n; d.a_k = 1; d.conjA = 1;
       d.B = G1 + (long)t0 * nn; d.b_k = 1; d.b_n.split = n; d.b_n.hi = nn; d.b_n.lo = n;
+      d.C = SB; d.c_m.lo = n; d.c_n.split = n; d.c_n.hi = Nnn; d.c_n.lo = 1;
       d.nb0 = kn;
-      d.a_b0 = Nnn; d.b_b0 = (long)T2 * nn;
-      SplitEmit em;
-      em.on = 1; em.side = 1; em.div_m = n; em.div_n = n; em.batch_from_n = 0;
-      em.k_b = nn; em.k_m = 1; em.k_n = n;
-      em.nkb = g.nkb; em.rows = g.ncol_pad; em.ex = eb; em.ex_ld = N; em.planes = b8;
-      c->launches += split_zgemm_emit(split, transposed(d), S, em, st);
+      d.a_b0 = Nnn; d.b_b0 = (long)T2 * nn; d.c_b0 = (long)tn * Nnn;
+      SplitRowMax mx;
+      mx.on = 1; mx.div_m = n; mx.div_n = n; mx.batch_from_n = 0; mx.ld = N; mx.ex = eb;
+      c->launches += split_zgemm_rowmax(split, transposed(d), S, mx, st);
     }
-    main(dm, a8, b8, ea, eb);
+    main(dm, ea, eb);
   }
 }
 
@@ -394,8 +361,7 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
   c->Gtmp.ensure((size_t)nk * ns * T * nn);
   double2* Vb = c->Vbuf.ensure((size_t)pl.kc * Nnn);
   double2* G1 = c->G1buf.ensure((size_t)pl.kc * T2 * nn);
-  const size_t scr = std::max(precision == GG_PREC_SPLIT ? (size_t)0 : (size_t)pl.kc * pl.tb * Nnn,
-                              (size_t)T * std::max(Nnn, NN));
+  const size_t scr = std::max((size_t)pl.kc * pl.tb * Nnn, (size_t)T * std::max(Nnn, NN));
   double2* SA = c->scratchA.ensure(scr);
   double2* SB = c->scratchB.ensure(scr);
   double2* P0 = c->P0buf.ensure((size_t)pl.qc * T2 * NN);
@@ -427,13 +393,11 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
     c->kstat_seconds[i] = 0.0;
     c->kstat_flops[i] = 0.0;
   }
-  struct Planes {
-    const int8_t* a8;
-    const int8_t* b8;
+  struct Exps {
     const int* ea;
     const int* eb;
   };
-  auto gemm_main = [&](ZgemmDesc d, int which, bool allow_split = true, const Planes* pr = nullptr) {
+  auto gemm_main = [&](ZgemmDesc d, int which, bool allow_split = true, const Exps* pr = nullptr) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c->profiling) {
       GG_CUDA(cudaEventCreate(&e0));
@@ -441,7 +405,9 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
       GG_CUDA(cudaEventRecord(e0, st));
     }
     if (split && pr) {
-      c->launches += split_zgemm_planes(split, d, c->slices, pr->a8, pr->b8, pr->ea, pr->eb, st);
+      d.work = gw_work;
+      d.work_elems = (long)c->gemm_work.n;
+      c->launches += split_zgemm_exps(split, d, c->slices, pr->ea, pr->eb, st);
     } else if (split && allow_split) {
       d.work = gw_work;
       d.work_elems = (long)c->gemm_work.n;
@@ -541,10 +507,9 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
                                G1, st);
           ++c->launches;
           if (split) {
-            p0_split_block(c, split, Gf, G1, Vb, P0 + (long)qi * T2 * NN, k0, kn, spin_a(sp), pl, pref,
-                           (sp == 0 && k0 == 0), st,
-                           [&](const ZgemmDesc& d, const int8_t* a8, const int8_t* b8, const int* ea, const int* eb) {
-                             const Planes pr{a8, b8, ea, eb};
+            p0_split_block(c, split, Gf, G1, Vb, SA, SB, P0 + (long)qi * T2 * NN, k0, kn, spin_a(sp), pl, pref,
+                           (sp == 0 && k0 == 0), st, [&](const ZgemmDesc& d, const int* ea, const int* eb) {
+                             const Exps pr{ea, eb};
                              gemm_main(d, 0, true, &pr);
                            });
             continue;

@@ -268,6 +268,7 @@ struct I8Args {
   int* err;
   SplitEmit em;            // em.on: the epilogue writes the product as int8 slices of another split
                            // GEMM's operand instead of writing C
+  SplitRowMax mx;          // mx.on: the epilogue also records the row maxima of C
   long long wait_cycles;   // limit of every barrier wait (WAIT_CYCLES; shorter in the time-out test)
   int skip_arrive;         // time-out test: CTA 0's first epilogue warp never releases the first
                            // drained accumulator, so the MMA warp's wait for it must run out
@@ -572,10 +573,41 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       // column offset c_n(n) stepped through the tile: (nq, nr) = divmod(n, split)
       const int csp = p.c_n.split > 0 ? p.c_n.split : 1 << 30;
       int nq = nbase / csp, nr = nbase - nq * csp;
+      // row maxima for the next GEMM: a run of columns with the same column key nq' is reduced
+      // per thread, then over the lanes with the same row key (consecutive lanes: a segmented
+      // warp reduction, the first lane of a segment does one atomicMax)
+      const int xkey = p.mx.on ? m / p.mx.div_m : 0;
+      int xq = p.mx.on ? nbase / p.mx.div_n : 0, xr = p.mx.on ? nbase - xq * p.mx.div_n : 0;
+      double xmax = 0.0;
+      auto xflush = [&](int colkey) {
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const double o = __shfl_down_sync(0xffffffffu, xmax, off);
+          const int ok = __shfl_down_sync(0xffffffffu, xkey, off);
+          if (lane + off < 32 && ok == xkey) xmax = fmax(xmax, o);
+        }
+        const int prev = __shfl_up_sync(0xffffffffu, xkey, 1);
+        if ((lane == 0 || prev != xkey) && xmax > 0.0) {
+          const long idx = p.mx.batch_from_n ? (long)colkey * p.mx.ld + xkey : (long)xkey * p.mx.ld + colkey;
+          atomicMax(p.mx.ex + idx, ilogb(xmax) + 1);
+        }
+        xmax = 0.0;
+      };
 #pragma unroll
       for (int c = 0; c < HC / 2; ++c) {
         const int eb = __shfl_sync(0xffffffffu, eb_lane, c);
         const int n = nbase + c;
+        if (p.mx.on) {
+          if (mok && n < p.N) {
+            const double sb = pow2i(eb + 2);
+            xmax = fmax(xmax, fmax(fabs(acc[2 * c] * sa * sb), fabs(acc[2 * c + 1] * sa * sb)));
+          }
+          if (++xr == p.mx.div_n) {
+            xflush(xq);
+            xr = 0;
+            ++xq;
+          }
+        }
         if (mok && n < p.N) {
           const double sb = pow2i(eb + 2);
           const double2 v = make_double2(acc[2 * c] * sa * sb, acc[2 * c + 1] * sa * sb);
@@ -593,6 +625,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           ++nq;
         }
       }
+      if (p.mx.on && xr != 0) xflush(xq);
     }
   }
   tc_fence_before();
@@ -942,7 +975,8 @@ Geometry geometry(const ZgemmDesc& d, int S) {
 
 // the persistent INT8 GEMM on operand planes (a8 / b8 of batch_a / batch_b batches)
 int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const int8_t* a8, const int8_t* b8,
-               const int* ea, const int* eb, bool a_shared, bool b_shared, const SplitEmit* em, cudaStream_t st) {
+               const int* ea, const int* eb, bool a_shared, bool b_shared, const SplitEmit* em, cudaStream_t st,
+               const SplitRowMax* mx = nullptr) {
   int* err = e->err.p;
   if (!err) {
     err = e->err.ensure(1);
@@ -977,6 +1011,7 @@ int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const
   a.beta = d.beta;
   a.err = err;
   if (em) a.em = *em;
+  if (mx) a.mx = *mx;
   a.wait_cycles = WAIT_CYCLES;
   a.skip_arrive = 0;
   if (e->timeout_test) {
@@ -999,7 +1034,7 @@ int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const
   // split-K so that the units fill whole waves of persistent CTAs (each split keeps >= 8 K
   // blocks); an emitting epilogue needs whole reductions (no split-K)
   int splits = 1;
-  if (!a.em.on) {
+  if (!a.em.on && !a.mx.on) {
     const int smax = (int)std::max<long>(1, std::min<long>(g.nkb / 8, 64));
     double best = 0.0;
     for (int sp = 1; sp <= smax; ++sp) {
@@ -1050,7 +1085,8 @@ int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const
 }
 
 // exponents and slices of both operands into the engine's planes, then the GEMM
-int sliced_gemm(SplitGemm* e, const ZgemmDesc& d, int S, const SplitEmit* em, cudaStream_t st) {
+int sliced_gemm(SplitGemm* e, const ZgemmDesc& d, int S, const SplitEmit* em, cudaStream_t st,
+                const SplitRowMax* mx = nullptr, const int* ea_given = nullptr, const int* eb_given = nullptr) {
   if (d.M <= 0 || d.N <= 0) return 0;
   const Geometry g = geometry(d, S);
   // an operand with zero batch strides is the same matrix for every batch: slice it once
@@ -1072,10 +1108,18 @@ int sliced_gemm(SplitGemm* e, const ZgemmDesc& d, int S, const SplitEmit* em, cu
       row_exponent_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(v, rows_pad, out, nb);
     GG_CHECK_LAUNCH();
   };
-  exponents(va, g.rows_a_pad, ea, batch_a);
-  exponents(vb, d.N, eb, batch_b);
+  int launches = 2;
+  if (ea_given && eb_given) {
+    if (a_shared || b_shared) throw Error(GG_ERR_ARG, "split: given exponents need per-batch operands");
+    ea = const_cast<int*>(ea_given);
+    eb = const_cast<int*>(eb_given);
+  } else {
+    exponents(va, g.rows_a_pad, ea, batch_a);
+    exponents(vb, d.N, eb, batch_b);
+    launches += 2;
+  }
   launch_slices(S, va, vb, g.rows_a_pad, g.ncol_pad, g.nkb, ea, eb, a8, b8, batch_a, batch_b, st);
-  return 4 + run_planes(e, d, S, g, a8, b8, ea, eb, a_shared, b_shared, em, st);
+  return launches + run_planes(e, d, S, g, a8, b8, ea, eb, a_shared, b_shared, em, st, mx);
 }
 
 }  // namespace
@@ -1101,6 +1145,19 @@ int split_zgemm_emit(SplitGemm* e, const ZgemmDesc& d, int S, const SplitEmit& e
   if (d.alpha.x != 1.0 || d.alpha.y != 0.0 || d.beta.x != 0.0 || d.beta.y != 0.0)
     throw Error(GG_ERR_ARG, "split emit: alpha must be 1 and beta 0");
   return sliced_gemm(e, d, S, &em, st);
+}
+
+int split_zgemm_rowmax(SplitGemm* e, const ZgemmDesc& d, int S, const SplitRowMax& mx, cudaStream_t st) {
+  if (!mx.on || !mx.ex || mx.div_m < 1 || mx.div_n < 1 || mx.ld < 1)
+    throw Error(GG_ERR_ARG, "split row max: incomplete target description");
+  if (d.alpha.x != 1.0 || d.alpha.y != 0.0 || d.beta.x != 0.0 || d.beta.y != 0.0)
+    throw Error(GG_ERR_ARG, "split row max: alpha must be 1 and beta 0");
+  return sliced_gemm(e, d, S, nullptr, st, &mx);
+}
+
+int split_zgemm_exps(SplitGemm* e, const ZgemmDesc& d, int S, const int* ea, const int* eb, cudaStream_t st) {
+  if (!ea || !eb) throw Error(GG_ERR_ARG, "split: exponents missing");
+  return sliced_gemm(e, d, S, nullptr, st, nullptr, ea, eb);
 }
 
 int split_zgemm_planes(SplitGemm* e, const ZgemmDesc& d, int S, const int8_t* a8, const int8_t* b8, const int* ea,

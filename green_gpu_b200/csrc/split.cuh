@@ -26,6 +26,19 @@ struct SplitEmit {
   int8_t* planes = nullptr;
 };
 
+// Epilogue that also records the exact row maxima of the product for the next split GEMM: with
+// m = mq div_m + mr and n = nq div_n + nr, |Re C|, |Im C| of (m, n) count towards entry
+// ex[nq * ld + mq] (batch_from_n) or ex[mq * ld + nq], which receives (by atomicMax over all
+// tiles and batches) the exponent e with max < 2^e - the exponent the slicing pass would compute
+// for that target row / column.  ex must start below every exponent (bytes 0x80).  No split-K.
+struct SplitRowMax {
+  int on = 0;
+  int div_m = 1, div_n = 1;
+  int batch_from_n = 0;
+  long ld = 0;
+  int* ex = nullptr;
+};
+
 // Geometry of a split GEMM's operand planes (as split_zgemm lays them out for descriptor d).
 struct SplitPlanes {
   int rows_a_pad = 0, rows_b_pad = 0, ncol_pad = 0;
@@ -42,6 +55,11 @@ SplitGemm* split_engine(gg_context* c);
 int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int slices, cudaStream_t st);
 // Same, with the epilogue writing slices of another operand (em.on = 1; no C written).
 int split_zgemm_emit(SplitGemm* e, const ZgemmDesc& d, int slices, const SplitEmit& em, cudaStream_t st);
+// Same as split_zgemm, recording the row maxima of C as described by mx (alpha = 1, beta = 0).
+int split_zgemm_rowmax(SplitGemm* e, const ZgemmDesc& d, int slices, const SplitRowMax& mx, cudaStream_t st);
+// split_zgemm with the operands' exponents given (ea [batch][rows_a_pad], eb [batch][N], as
+// split_zgemm_rowmax records them): only the slicing pass and the GEMM run.
+int split_zgemm_exps(SplitGemm* e, const ZgemmDesc& d, int slices, const int* ea, const int* eb, cudaStream_t st);
 // The GEMM of descriptor d (d.A / d.B unused) on operands already in planes of geometry
 // split_planes_for(d, slices), with exponents ea [batch][rows_a_pad] and eb [batch][N].
 int split_zgemm_planes(SplitGemm* e, const ZgemmDesc& d, int slices, const int8_t* a8, const int8_t* b8,
