@@ -576,21 +576,20 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       // row maxima for the next GEMM: a run of columns with the same column key nq' is reduced
       // per thread, then over the lanes with the same row key (consecutive lanes: a segmented
       // warp reduction, the first lane of a segment does one atomicMax)
-      const int xkey = p.mx.on ? m / p.mx.div_m : 0;
+      const int xmq = p.mx.on ? m / p.mx.div_m : 0, xmr = m - xmq * p.mx.div_m;
+      const long xrow = w.batch * p.mx.s_b + xmq * p.mx.s_mq + xmr * p.mx.s_mr;
       int xq = p.mx.on ? nbase / p.mx.div_n : 0, xr = p.mx.on ? nbase - xq * p.mx.div_n : 0;
       double xmax = 0.0;
       auto xflush = [&](int colkey) {
+        const long idx = xrow + colkey * p.mx.s_nq;
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
           const double o = __shfl_down_sync(0xffffffffu, xmax, off);
-          const int ok = __shfl_down_sync(0xffffffffu, xkey, off);
-          if (lane + off < 32 && ok == xkey) xmax = fmax(xmax, o);
+          const long oi = __shfl_down_sync(0xffffffffu, idx, off);
+          if (lane + off < 32 && oi == idx) xmax = fmax(xmax, o);
         }
-        const int prev = __shfl_up_sync(0xffffffffu, xkey, 1);
-        if ((lane == 0 || prev != xkey) && xmax > 0.0) {
-          const long idx = p.mx.batch_from_n ? (long)colkey * p.mx.ld + xkey : (long)xkey * p.mx.ld + colkey;
-          atomicMax(p.mx.ex + idx, ilogb(xmax) + 1);
-        }
+        const long prev = __shfl_up_sync(0xffffffffu, idx, 1);
+        if ((lane == 0 || prev != idx) && xmax > 0.0) atomicMax(p.mx.ex + idx, ilogb(xmax) + 1);
         xmax = 0.0;
       };
 #pragma unroll
@@ -1109,14 +1108,19 @@ int sliced_gemm(SplitGemm* e, const ZgemmDesc& d, int S, const SplitEmit* em, cu
     GG_CHECK_LAUNCH();
   };
   int launches = 2;
-  if (ea_given && eb_given) {
-    if (a_shared || b_shared) throw Error(GG_ERR_ARG, "split: given exponents need per-batch operands");
+  if ((ea_given && a_shared) || (eb_given && b_shared))
+    throw Error(GG_ERR_ARG, "split: given exponents need per-batch operands");
+  if (ea_given) {
     ea = const_cast<int*>(ea_given);
-    eb = const_cast<int*>(eb_given);
   } else {
     exponents(va, g.rows_a_pad, ea, batch_a);
+    ++launches;
+  }
+  if (eb_given) {
+    eb = const_cast<int*>(eb_given);
+  } else {
     exponents(vb, d.N, eb, batch_b);
-    launches += 2;
+    ++launches;
   }
   launch_slices(S, va, vb, g.rows_a_pad, g.ncol_pad, g.nkb, ea, eb, a8, b8, batch_a, batch_b, st);
   return launches + run_planes(e, d, S, g, a8, b8, ea, eb, a_shared, b_shared, em, st, mx);
@@ -1148,16 +1152,18 @@ int split_zgemm_emit(SplitGemm* e, const ZgemmDesc& d, int S, const SplitEmit& e
 }
 
 int split_zgemm_rowmax(SplitGemm* e, const ZgemmDesc& d, int S, const SplitRowMax& mx, cudaStream_t st) {
-  if (!mx.on || !mx.ex || mx.div_m < 1 || mx.div_n < 1 || mx.ld < 1)
+  if (!mx.on || !mx.ex || mx.div_m < 1 || mx.div_n < 1)
     throw Error(GG_ERR_ARG, "split row max: incomplete target description");
   if (d.alpha.x != 1.0 || d.alpha.y != 0.0 || d.beta.x != 0.0 || d.beta.y != 0.0)
     throw Error(GG_ERR_ARG, "split row max: alpha must be 1 and beta 0");
   return sliced_gemm(e, d, S, nullptr, st, &mx);
 }
 
-int split_zgemm_exps(SplitGemm* e, const ZgemmDesc& d, int S, const int* ea, const int* eb, cudaStream_t st) {
-  if (!ea || !eb) throw Error(GG_ERR_ARG, "split: exponents missing");
-  return sliced_gemm(e, d, S, nullptr, st, nullptr, ea, eb);
+int split_zgemm_exps(SplitGemm* e, const ZgemmDesc& d, int S, const int* ea, const int* eb, cudaStream_t st,
+                     const SplitRowMax* mx) {
+  if (mx && (d.alpha.x != 1.0 || d.alpha.y != 0.0 || d.beta.x != 0.0 || d.beta.y != 0.0))
+    throw Error(GG_ERR_ARG, "split row max: alpha must be 1 and beta 0");
+  return sliced_gemm(e, d, S, nullptr, st, mx, ea, eb);
 }
 
 int split_zgemm_planes(SplitGemm* e, const ZgemmDesc& d, int S, const int8_t* a8, const int8_t* b8, const int* ea,

@@ -27,15 +27,15 @@ struct SplitEmit {
 };
 
 // Epilogue that also records the exact row maxima of the product for the next split GEMM: with
-// m = mq div_m + mr and n = nq div_n + nr, |Re C|, |Im C| of (m, n) count towards entry
-// ex[nq * ld + mq] (batch_from_n) or ex[mq * ld + nq], which receives (by atomicMax over all
+// m = mq div_m + mr and n = nq div_n + nr, |Re C|, |Im C| of (m, n) of batch b count towards
+// entry ex[b * s_b + mq * s_mq + mr * s_mr + nq * s_nq], which receives (by atomicMax over all
 // tiles and batches) the exponent e with max < 2^e - the exponent the slicing pass would compute
-// for that target row / column.  ex must start below every exponent (bytes 0x80).  No split-K.
+// for that row / column of the next GEMM's operand.  ex must start below every exponent (bytes
+// 0x80).  No split-K.
 struct SplitRowMax {
   int on = 0;
   int div_m = 1, div_n = 1;
-  int batch_from_n = 0;
-  long ld = 0;
+  long s_b = 0, s_mq = 0, s_mr = 0, s_nq = 0;
   int* ex = nullptr;
 };
 
@@ -57,9 +57,11 @@ int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int slices, cudaStream_t st);
 int split_zgemm_emit(SplitGemm* e, const ZgemmDesc& d, int slices, const SplitEmit& em, cudaStream_t st);
 // Same as split_zgemm, recording the row maxima of C as described by mx (alpha = 1, beta = 0).
 int split_zgemm_rowmax(SplitGemm* e, const ZgemmDesc& d, int slices, const SplitRowMax& mx, cudaStream_t st);
-// split_zgemm with the operands' exponents given (ea [batch][rows_a_pad], eb [batch][N], as
-// split_zgemm_rowmax records them): only the slicing pass and the GEMM run.
-int split_zgemm_exps(SplitGemm* e, const ZgemmDesc& d, int slices, const int* ea, const int* eb, cudaStream_t st);
+// split_zgemm with operand exponents given (ea [batch][rows_a_pad], eb [batch][N], as
+// split_zgemm_rowmax records them; NULL: computed by the exponent pass as usual), optionally
+// recording the row maxima of its own product (mx may be NULL).
+int split_zgemm_exps(SplitGemm* e, const ZgemmDesc& d, int slices, const int* ea, const int* eb, cudaStream_t st,
+                     const SplitRowMax* mx = nullptr);
 // The GEMM of descriptor d (d.A / d.B unused) on operands already in planes of geometry
 // split_planes_for(d, slices), with exponents ea [batch][rows_a_pad] and eb [batch][N].
 int split_zgemm_planes(SplitGemm* e, const ZgemmDesc& d, int slices, const int8_t* a8, const int8_t* b8,
