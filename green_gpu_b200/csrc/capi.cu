@@ -287,7 +287,7 @@ std::vector<const void*> gg_context::buffer_signature() const {
                                 Vbuf.p,  G1buf.p,   scratchA.p, scratchB.p, P0buf.p, Pw.p,     Afac.p,
                                 Wt.p,    Wrot.p,    gemm_work.p, hf_D.p,  hf_F.p,      hf_c.p,     hf_J.p,
                                 info.p,  piv.p,     idx_i.p,   pos_d.p,  op_d.p,      gw_err.p,   gw_tables.get(),
-                                p0_ea.p, p0_eb.p,   sg_xexp.p, sg_zexp.p};
+                                p0_ea.p, p0_eb.p};
   split_buffers(split, v);
   return v;
 }

@@ -100,9 +100,6 @@ struct gg_context {
   // split precision: exponents of the P0 main contraction's operand rows / columns, recorded
   // by the operand builds' epilogues
   gg::DevBuf<int> p0_ea, p0_eb;
-  // split precision: exponents of the Sigma steps' operands X (rows (Q, j) per tau) and Z (rows
-  // (tau, j)), recorded by the epilogues of the GEMMs that produce them
-  gg::DevBuf<int> sg_xexp, sg_zexp;
   gg::DevBuf<int64_t> pos_d;
   gg::DevBuf<int> op_d;
 

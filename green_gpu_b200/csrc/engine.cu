@@ -651,32 +651,6 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
           const int k1 = (int)c->k2_from_k1q[(size_t)c->k_r2f[kr] * s.nq + qd];
           sg_pairs.gather(c, (size_t)qd * s.ink + kr, 1, Vb, st);
           ++c->launches;
-          // the two steps after the main contraction (X G and Z V^+) and their operands' row
-          // exponents: in split precision both run on the INT8 engine, each with the exact
-          // exponents of its large operand recorded by the epilogue of the GEMM that made it, so
-          // no exponent scan of X or Z is needed (only their slicing passes)
-          ZgemmDesc dxg;  // Z[t][Q][j][c] = sum_l X[t][Q][j][l] G^{k1}(tau_t)[l][c]
-          dxg.M = N * n; dxg.N = n; dxg.K = n;
-          dxg.A = SA; dxg.a_m.lo = n; dxg.a_k = 1;
-          dxg.b_k = n; dxg.b_n.lo = 1;
-          dxg.C = SB; dxg.c_m.lo = n; dxg.c_n.lo = 1;
-          dxg.nb0 = T; dxg.a_b0 = Nnn; dxg.b_b0 = nn; dxg.c_b0 = Nnn;
-          ZgemmDesc dzv;  // Sigma[t][sp][kr][j][i] += -1/nk sum_{Q,c} Z[t][Q][j][c] conj(V[Q][i][c])
-          dzv.M = T * n; dzv.N = n; dzv.K = n; dzv.KB = N;
-          dzv.A = SB; dzv.a_m.split = n; dzv.a_m.hi = Nnn; dzv.a_m.lo = n; dzv.a_k = 1; dzv.a_kb = nn;
-          dzv.B = Vb; dzv.b_k = 1; dzv.b_n.lo = n; dzv.b_kb = nn; dzv.conjB = 1;
-          dzv.c_m.split = n; dzv.c_m.hi = (long)ns * s.ink * nn; dzv.c_m.lo = n; dzv.c_n.lo = 1;
-          dzv.alpha = make_double2(-1.0 / nk, 0.0);
-          dzv.beta = make_double2(1.0, 0.0);
-          int* xexp = nullptr;
-          int* zexp = nullptr;
-          long xld = 0;
-          if (split) {
-            xld = split_planes_for(dxg, c->slices).rows_a_pad;
-            xexp = c->sg_xexp.ensure((size_t)T * xld);
-            zexp = c->sg_zexp.ensure((size_t)split_planes_for(dzv, c->slices).rows_a_pad);
-            GG_CUDA(cudaMemsetAsync(xexp, 0x80, sizeof(int) * (size_t)T * xld, st));
-          }
           // X[t][Q][j][l] = sum_P V[P][j][l] W'[t][P][Q]; W' = conj(W) for TR partners.  Rows are
           // x = (j, l), columns Q.  V does not depend on tau or spin: it is the shared operand
           // of the tau batch (sliced once in split precision) and X serves every spin.
@@ -687,29 +661,33 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
             d.B = W; d.b_k = N; d.b_n.lo = 1; d.conjB = trq ? 1 : 0;
             d.C = SA; d.c_m.lo = 1; d.c_n.lo = nn;
             d.nb0 = T; d.a_b0 = 0; d.b_b0 = NN; d.c_b0 = Nnn;
-            // X row (Q, j) of batch t for the X G step: m = (j, l) -> j = mq, n = Q
-            SplitRowMax mx;
-            mx.on = 1; mx.div_m = n; mx.div_n = 1; mx.s_b = xld; mx.s_mq = 1; mx.s_nq = n; mx.ex = xexp;
-            gemm_main(d, 1, true, nullptr, split ? &mx : nullptr);
+            gemm_main(d, 1);
           }
           for (int sp = 0; sp < ns; ++sp) {
-            ZgemmDesc d = dxg;
-            d.B = Gf + ((long)k1 * ns + sp) * T * nn;
-            ZgemmDesc e = dzv;
-            e.C = Sigma_dev + ((long)sp * s.ink + kr) * nn;
-            if (split) {
-              // Z row (t, j) for the Z V^+ step: m = (Q, j) -> j = mr, batch t
-              GG_CUDA(cudaMemsetAsync(zexp, 0x80, sizeof(int) * c->sg_zexp.n, st));
-              SplitRowMax mz;
-              mz.on = 1; mz.div_m = n; mz.div_n = 1 << 30; mz.s_b = n; mz.s_mr = 1; mz.ex = zexp;
-              d.work = gw_work;
-              d.work_elems = (long)c->gemm_work.n;
-              c->launches += split_zgemm_exps(split, d, c->slices, xexp, nullptr, st, &mz);
-              const Exps ez{zexp, nullptr};
-              gemm_main(e, 2, true, &ez);
-            } else {
+            // Z[t][Q][j][c] = sum_l X[t][Q][j][l] G^{k1}(tau_t)[l][c]
+            {
+              ZgemmDesc d;
+              d.M = N * n; d.N = n; d.K = n;
+              d.A = SA; d.a_m.lo = n; d.a_k = 1;
+              d.B = Gf + ((long)k1 * ns + sp) * T * nn; d.b_k = n; d.b_n.lo = 1;
+              d.C = SB; d.c_m.lo = n; d.c_n.lo = 1;
+              d.nb0 = T; d.a_b0 = Nnn; d.b_b0 = nn; d.c_b0 = Nnn;
               gemm(d);
-              gemm_main(e, 2, false);
+            }
+            // Sigma[t][sp][kr][j][i] += -1/nk sum_Q sum_c Z[t][Q][j][c] conj(V[Q][i][c])
+            // (one GEMM over all tau: rows m = (t, j), V is the shared operand).  FP64 in both
+            // precisions: on the INT8 engine these two steps (and the slicing of X and Z, new
+            // for every tau) measured slower than the FP64 tensor cores
+            {
+              ZgemmDesc d;
+              d.M = T * n; d.N = n; d.K = n; d.KB = N;
+              d.A = SB; d.a_m.split = n; d.a_m.hi = Nnn; d.a_m.lo = n; d.a_k = 1; d.a_kb = nn;
+              d.B = Vb; d.b_k = 1; d.b_n.lo = n; d.b_kb = nn; d.conjB = 1;
+              d.C = Sigma_dev + ((long)sp * s.ink + kr) * nn;
+              d.c_m.split = n; d.c_m.hi = (long)ns * s.ink * nn; d.c_m.lo = n; d.c_n.lo = 1;
+              d.alpha = make_double2(-1.0 / nk, 0.0);
+              d.beta = make_double2(1.0, 0.0);
+              gemm_main(d, 2, false);
             }
           }
         }

@@ -513,7 +513,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       for (int i = 0; i < HC; ++i) acc[i] = 0.0;
       // one drain per K segment: segments end at kb1 and at every multiple of kcb
       for (int k0 = w.kb0; k0 < w.kb1 && ok; k0 = min(w.kb1, (k0 / p.kcb + 1) * p.kcb)) {
-#pragma unroll
+        // a runtime loop over the diagonals: one copy of the drain code instead of S (the
+        // unrolled form made the epilogue larger than the instruction cache, which stalled
+        // the short-K GEMMs whose epilogue runs after every two K blocks)
+#pragma unroll 1
         for (int d = 2; d <= S + 1; ++d) {
           if (!mbar_wait(&accf[buf * ND + d - 2], par, err, 8, p.wait_cycles)) { ok = false; break; }
           tc_fence_after();
@@ -573,31 +576,31 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       // column offset c_n(n) stepped through the tile: (nq, nr) = divmod(n, split)
       const int csp = p.c_n.split > 0 ? p.c_n.split : 1 << 30;
       int nq = nbase / csp, nr = nbase - nq * csp;
-      // row maxima for the next GEMM: a run of columns with the same column key nq' is reduced
-      // per thread, then over the lanes with the same row key (consecutive lanes: a segmented
-      // warp reduction, the first lane of a segment does one atomicMax)
-      const int xmq = p.mx.on ? m / p.mx.div_m : 0, xmr = m - xmq * p.mx.div_m;
-      const long xrow = w.batch * p.mx.s_b + xmq * p.mx.s_mq + xmr * p.mx.s_mr;
-      int xq = p.mx.on ? nbase / p.mx.div_n : 0, xr = p.mx.on ? nbase - xq * p.mx.div_n : 0;
-      double xmax = 0.0;
-      auto xflush = [&](int colkey) {
-        const long idx = xrow + colkey * p.mx.s_nq;
+      if (p.mx.on) {
+        // row maxima for the next GEMM (kept out of the store loop below, whose code stays
+        // compact): a run of columns with the same column key is reduced per thread, then over
+        // the lanes with the same target row (consecutive lanes: a segmented warp reduction;
+        // the first lane of a segment does one atomicMax)
+        const int xmq = m / p.mx.div_m, xmr = m - xmq * p.mx.div_m;
+        const long xrow = w.batch * p.mx.s_b + xmq * p.mx.s_mq + xmr * p.mx.s_mr;
+        int xq = nbase / p.mx.div_n, xr = nbase - xq * p.mx.div_n;
+        double xmax = 0.0;
+        auto xflush = [&](int colkey) {
+          const long idx = xrow + colkey * p.mx.s_nq;
 #pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-          const double o = __shfl_down_sync(0xffffffffu, xmax, off);
-          const long oi = __shfl_down_sync(0xffffffffu, idx, off);
-          if (lane + off < 32 && oi == idx) xmax = fmax(xmax, o);
-        }
-        const long prev = __shfl_up_sync(0xffffffffu, idx, 1);
-        if ((lane == 0 || prev != idx) && xmax > 0.0) atomicMax(p.mx.ex + idx, ilogb(xmax) + 1);
-        xmax = 0.0;
-      };
+          for (int off = 1; off < 32; off <<= 1) {
+            const double o = __shfl_down_sync(0xffffffffu, xmax, off);
+            const long oi = __shfl_down_sync(0xffffffffu, idx, off);
+            if (lane + off < 32 && oi == idx) xmax = fmax(xmax, o);
+          }
+          const long prev = __shfl_up_sync(0xffffffffu, idx, 1);
+          if ((lane == 0 || prev != idx) && xmax > 0.0) atomicMax(p.mx.ex + idx, ilogb(xmax) + 1);
+          xmax = 0.0;
+        };
 #pragma unroll
-      for (int c = 0; c < HC / 2; ++c) {
-        const int eb = __shfl_sync(0xffffffffu, eb_lane, c);
-        const int n = nbase + c;
-        if (p.mx.on) {
-          if (mok && n < p.N) {
+        for (int c = 0; c < HC / 2; ++c) {
+          const int eb = __shfl_sync(0xffffffffu, eb_lane, c);
+          if (mok && nbase + c < p.N) {
             const double sb = pow2i(eb + 2);
             xmax = fmax(xmax, fmax(fabs(acc[2 * c] * sa * sb), fabs(acc[2 * c + 1] * sa * sb)));
           }
@@ -607,6 +610,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             ++xq;
           }
         }
+        if (xr != 0) xflush(xq);
+      }
+#pragma unroll
+      for (int c = 0; c < HC / 2; ++c) {
+        const int eb = __shfl_sync(0xffffffffu, eb_lane, c);
+        const int n = nbase + c;
         if (mok && n < p.N) {
           const double sb = pow2i(eb + 2);
           const double2 v = make_double2(acc[2 * c] * sa * sb, acc[2 * c + 1] * sa * sb);
@@ -624,7 +633,6 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           ++nq;
         }
       }
-      if (p.mx.on && xr != 0) xflush(xq);
     }
   }
   tc_fence_before();
