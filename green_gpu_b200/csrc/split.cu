@@ -97,10 +97,10 @@ __device__ __forceinline__ bool mbar_try_sleep(uint64_t* b, uint32_t parity, uin
   return ok != 0;
 }
 // bounded wait; returns false (and records `code`) on time-out or when another role failed
-// (abort_on_err = false for the teardown waits that must see in-flight work complete)
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* err, int code, long long limit,
-                                          bool abort_on_err = true) {
-  if (mbar_try(b, parity)) return true;  // fast path: no clock read when the phase is complete
+// (abort_on_err = false for the teardown waits that must see in-flight work complete).  The
+// polling loop is a separate function so that the many inlined waits stay small.
+__device__ __noinline__ bool mbar_wait_slow(uint64_t* b, uint32_t parity, volatile int* err, int code, long long limit,
+                                            bool abort_on_err) {
   const long long t0 = clock64();
   while (!mbar_try_sleep(b, parity, 100000)) {  // <= 0.1 ms per suspension
     if (abort_on_err && *err) return false;
@@ -110,6 +110,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile
     }
   }
   return true;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* err, int code, long long limit,
+                                          bool abort_on_err = true) {
+  if (mbar_try(b, parity)) return true;  // fast path: no clock read when the phase is complete
+  return mbar_wait_slow(b, parity, err, code, limit, abort_on_err);
 }
 
 // box {64 bytes, rows, 1} at (0, row, plane); the innermost coordinate is always 0.
@@ -184,6 +190,29 @@ __device__ __forceinline__ double pow2i(int e) {
 // 2^e for e in the normal range (exact)
 __device__ __forceinline__ double scale_pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
 
+// Base-128 digits of an integer |X| <= 2^(7S-1): the lower S - 1 balanced in [-63, 64], the
+// top one the remaining quotient (|d_1| <= 64), so X = sum_s d_s 128^(S-s) exactly.
+template <int S>
+__device__ __forceinline__ void digits(long long X, int8_t* d) {
+#pragma unroll
+  for (int s = S - 1; s >= 1; --s) {
+    int r = (int)(X & 127);
+    r -= (r > 64) ? 128 : 0;
+    d[s] = (int8_t)r;
+    X = (X - r) >> 7;
+  }
+  d[0] = (int8_t)X;
+}
+
+// cut x (|x| < 1 after scaling) into S int8 slices: X = rint(x 2^(7S-1)) (one rounding, to
+// nearest even) split into digits, so x = 2 sum_s d_s 2^-7s + O(2^-7S) with every |d_s| <= 64
+// and an unbiased residual.  Integer arithmetic after one conversion (a chain of FP64
+// roundings per slice made the slicing pass compute-bound).
+template <int S>
+__device__ __forceinline__ void cut(double x, int8_t* d) {
+  digits<S>(__double2ll_rn(x * (double)(1LL << (7 * S - 1))), d);
+}
+
 // drain `NC` int32 columns (a multiple of 8, at most 32) starting at taddr into acc * scale
 template <int NC>
 __device__ __forceinline__ void drain_cols(uint32_t taddr, double* acc, double scale) {
@@ -210,20 +239,9 @@ __device__ __forceinline__ void drain_cols(uint32_t taddr, double* acc, double s
 template <int S>
 __device__ __forceinline__ void emit_slices(double2 v, int e, const SplitEmit& em, long tb, int tr, long k) {
   const double f = scale_pow2(7 * S - 1 - e);
-  long long xr = __double2ll_rn(v.x * f), xi = __double2ll_rn(v.y * f);
   int8_t dr[S], di[S];
-#pragma unroll
-  for (int s = S - 1; s >= 1; --s) {
-    int r = (int)(xr & 127), i = (int)(xi & 127);
-    r -= (r > 64) ? 128 : 0;
-    i -= (i > 64) ? 128 : 0;
-    dr[s] = (int8_t)r;
-    di[s] = (int8_t)i;
-    xr = (xr - r) >> 7;
-    xi = (xi - i) >> 7;
-  }
-  dr[0] = (int8_t)xr;
-  di[0] = (int8_t)xi;
+  digits<S>(__double2ll_rn(v.x * f), dr);
+  digits<S>(__double2ll_rn(v.y * f), di);
   const long kb = k >> 5;
   const int off = 2 * (int)(k & 31);
   if (em.side == 0) {
@@ -300,11 +318,13 @@ __device__ __forceinline__ Unit unit_of(const I8Args& p, long u, int BN) {
 // overwrites it, and with `reuse` it first waits until the epilogue has drained that
 // diagonal); LAST: the last K block (a commit per diagonal tells the epilogue that the
 // diagonal is complete).  Descriptor offsets are compile-time constants.
+// (A runtime loop: these first / last K blocks of a segment are few per tile, and unrolled
+// copies of them made the kernel larger than the instruction cache.)
 template <int S, int BN, bool FIRST, bool LAST>
 __device__ __forceinline__ bool issue_kblock(uint32_t tacc0, uint64_t da, uint64_t db, uint32_t idesc, uint32_t leader,
                                              bool reuse, uint64_t* acce, uint64_t* accf, uint32_t par_e,
                                              volatile int* err, long long limit) {
-#pragma unroll
+#pragma unroll 1
   for (int d = 2; d <= S + 1; ++d) {
     if (FIRST && reuse) {
       if (!__all_sync(0xffffffffu, mbar_wait(&acce[d - 2], par_e, err, 2, limit))) return false;
@@ -312,14 +332,15 @@ __device__ __forceinline__ bool issue_kblock(uint32_t tacc0, uint64_t da, uint64
     }
     const uint32_t tacc = tacc0 + (uint32_t)((d - 2) * BN);
     const int s_lo = d - S > 1 ? d - S : 1, s_hi = d - 1 < S ? d - 1 : S;
-#pragma unroll
+#pragma unroll 1
     for (int s = s_lo; s <= s_hi; ++s) {
       const int t = d - s;
+      const uint64_t a = da + (uint64_t)(((s - 1) * BM * KB) >> 4);
+      const uint64_t b = db + (uint64_t)(((t - 1) * BN * KB) >> 4);
 #pragma unroll
       for (int kk = 0; kk < KB / 32; ++kk)
-        mma_i8(tacc, da + (uint64_t)(((s - 1) * BM * KB) >> 4) + (uint64_t)(kk * 2),
-               db + (uint64_t)(((t - 1) * BN * KB) >> 4) + (uint64_t)(kk * 2), idesc,
-               (FIRST && s == s_lo && kk == 0) ? 0u : 1u, leader);
+        mma_i8(tacc, a + (uint64_t)(kk * 2), b + (uint64_t)(kk * 2), idesc, (FIRST && s == s_lo && kk == 0) ? 0u : 1u,
+               leader);
     }
     if (LAST) mma_commit(&accf[d - 2], leader);
   }
@@ -716,24 +737,6 @@ __global__ void row_exponent_rc_kernel(OpView v, int rows_pad, int* out, long nb
   out[gt] = mx > 0.0 ? ilogb(mx) + 1 : 0;
 }
 
-// cut x (|x| < 1 after scaling) into S int8 slices by rounding to nearest:
-// d_1 = rint(64 x), r_1 = 64 x - d_1 in [-1/2, 1/2]; d_s = rint(128 r_{s-1}), ...
-// so x = 2 sum_s d_s 2^-7s + O(2^-7S), every |d_s| <= 64 and the residual is unbiased.
-// rint is done by adding 2^52 + 2^51 (the sum is rounded to an integer, round-to-nearest-
-// even like rint, and its low word holds that integer in two's complement); every step is
-// exact in FP64 and uses only the add / fma pipes.
-template <int S>
-__device__ __forceinline__ void cut(double x, int8_t* d) {
-  const double RND = 6755399441055744.0;  // 2^52 + 2^51
-  x *= 64.0;
-#pragma unroll
-  for (int s = 0; s < S; ++s) {
-    const double y = x + RND;
-    d[s] = (int8_t)__double2loint(y);
-    const double t = y - RND;
-    x = (x - t) * 128.0;
-  }
-}
 
 // x * 2^-e, exact while the result is a normal number (ldexp outside the directly encodable range)
 __device__ __forceinline__ double scale_neg(double x, int e) {
