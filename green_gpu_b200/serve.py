@@ -14,7 +14,8 @@ Scheduling:
   resident integrals plus the un-chunked work space) fits the free part of the memory
   budget; jobs that could never fit are rejected with the reason;
 * admitted jobs run concurrently, each on its own context and CUDA stream, so their
-  kernels overlap on the device; a finished job frees its slot and its memory at once
+  kernels can overlap on the device (``serve_bench --overlap`` measures it: the same stream
+  with one slot and with several); a finished job frees its slot and its memory at once
   and the queue is re-examined (continuous batching, not a run-to-completion queue).
 
 ``Server.stats()`` reports per-job latency (arrival to last iteration) p50 / p99,
