@@ -96,64 +96,6 @@ __global__ void transpose_blocks_kernel(const double2* __restrict__ in, int n, i
   }
 }
 
-// one block of 64 threads per matrix: thread a < n takes the norm of row a and of column a
-__global__ void norm_max_kernel(const double2* __restrict__ base, int ni, long so, long si, int n,
-                                double* __restrict__ row_max, double* __restrict__ col_max) {
-  const int o = blockIdx.x / ni, i = blockIdx.x % ni;
-  const double2* M = base + o * so + i * si;
-  double rmax = 0.0, cmax = 0.0;
-  for (int a = threadIdx.x; a < n; a += blockDim.x) {
-    double r = 0.0, c = 0.0;
-    for (int j = 0; j < n; ++j) {
-      const double2 x = M[(long)a * n + j];
-      r = fma(x.x, x.x, fma(x.y, x.y, r));
-      if (col_max) {
-        const double2 y = M[(long)j * n + a];
-        c = fma(y.x, y.x, fma(y.y, y.y, c));
-      }
-    }
-    rmax = fmax(rmax, r);
-    cmax = fmax(cmax, c);
-  }
-  for (int off = 16; off > 0; off >>= 1) {
-    rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, off));
-    cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, off));
-  }
-  __shared__ double sr[2], sc[2];
-  if ((threadIdx.x & 31) == 0) {
-    sr[threadIdx.x >> 5] = rmax;
-    sc[threadIdx.x >> 5] = cmax;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    row_max[blockIdx.x] = sqrt(fmax(sr[0], sr[1]));
-    if (col_max) col_max[blockIdx.x] = sqrt(fmax(sc[0], sc[1]));
-  }
-}
-
-__global__ void bound_exponents_kernel(const double* __restrict__ g, const double* __restrict__ v, int nk, int nt,
-                                       int nr, int ld, int* __restrict__ ex) {
-  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i >= (long)nt * ld) return;
-  const int t = (int)(i / ld), r = (int)(i % ld);
-  int e = 0;
-  if (r < nr) {
-    double B = 0.0;
-    for (int k = 0; k < nk; ++k) B = fmax(B, g[(long)k * nt + t] * v[(long)k * nr + r]);
-    // the factor covers the rounding of the bound and of the product the bound applies to
-    e = B > 0.0 ? ilogb(B * (1.0 + 0x1p-20)) + 1 : 0;
-  }
-  ex[i] = e;
-}
-
-__global__ void zero_kpad_kernel(int8_t* planes, long slabs, long nkb, long rows, int valid) {
-  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i >= slabs * rows) return;
-  const long slab = i / rows, r = i % rows;
-  int8_t* row = planes + (((slab * nkb + nkb - 1) * rows + r) << 6);
-  for (int b = valid; b < 64; ++b) row[b] = 0;
-}
-
 __global__ void axpy_kernel(double2* y, const double2* x, long n) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
     y[i] = cadd(y[i], x[i]);
@@ -649,30 +591,6 @@ void launch_transpose_blocks(const double2* in, long nblocks, int n, double2* ou
   if (nblocks > 65535) throw Error(GG_ERR_ARG, "transpose: too many blocks for one launch");
   const int tiles = (n + 31) / 32;
   transpose_blocks_kernel<<<dim3((unsigned)(tiles * tiles), (unsigned)nblocks), dim3(32, 8), 0, st>>>(in, n, tiles, out);
-  GG_CHECK_LAUNCH();
-}
-
-void launch_norm_max(const double2* base, int no, long so, int ni, long si, int n, double* row_max, double* col_max,
-                     cudaStream_t st) {
-  const long blocks = (long)no * ni;
-  if (blocks <= 0) return;
-  if (blocks > 0x7fffffffL || n > 4096) throw Error(GG_ERR_ARG, "norm_max: too many or too large matrices");
-  norm_max_kernel<<<(unsigned)blocks, 64, 0, st>>>(base, ni, so, si, n, row_max, col_max);
-  GG_CHECK_LAUNCH();
-}
-
-void launch_bound_exponents(const double* g, const double* v, int nk, int nt, int nr, int ld, int* ex,
-                            cudaStream_t st) {
-  const long total = (long)nt * ld;
-  if (total <= 0) return;
-  bound_exponents_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(g, v, nk, nt, nr, ld, ex);
-  GG_CHECK_LAUNCH();
-}
-
-void launch_zero_kpad(int8_t* planes, long slabs, long nkb, long rows, int valid, cudaStream_t st) {
-  const long total = slabs * rows;
-  if (total <= 0 || valid >= 64) return;
-  zero_kpad_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(planes, slabs, nkb, rows, valid);
   GG_CHECK_LAUNCH();
 }
 

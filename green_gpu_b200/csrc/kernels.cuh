@@ -40,20 +40,6 @@ void launch_x2c_merge(const double2* in, long nouter, long ninner, int n, int nb
 // out[b][i][j] = in[b][j][i] for nblocks n x n matrices (32 x 32 tiles through shared memory)
 void launch_transpose_blocks(const double2* in, long nblocks, int n, double2* out, cudaStream_t st);
 
-// Norm maxima of n x n row-major matrices M(o, i) = base + o * so + i * si (o < no, i < ni):
-// row_max[o * ni + i] = max_a ||M[a, :]||_2 and, if col_max is not NULL,
-// col_max[o * ni + i] = max_b ||M[:, b]||_2.
-void launch_norm_max(const double2* base, int no, long so, int ni, long si, int n, double* row_max, double* col_max,
-                     cudaStream_t st);
-// Exponent bounds of a product operand: ex[t * ld + r] = e(max_k g[k * nt + t] * v[k * nr + r]) for
-// r < nr, 0 for nr <= r < ld, where e(B) = ilogb(B (1 + 2^-20)) + 1 (0 for B = 0), so that every
-// element bounded by B has |x| < 2^e.
-void launch_bound_exponents(const double* g, const double* v, int nk, int nt, int nr, int ld, int* ex,
-                            cudaStream_t st);
-// Zero the bytes [valid, 64) of every row of the last K block of each of `slabs` slabs of nkb
-// planes (rows x 64 bytes each): the K padding of operand planes written element by element.
-void launch_zero_kpad(int8_t* planes, long slabs, long nkb, long rows, int valid, cudaStream_t st);
-
 // scale: X *= s
 void launch_scale(double2* X, long n, double s, cudaStream_t st);
 void launch_fill_zero(double2* X, long n, cudaStream_t st);

@@ -190,29 +190,6 @@ __device__ __forceinline__ double pow2i(int e) {
 // 2^e for e in the normal range (exact)
 __device__ __forceinline__ double scale_pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
 
-// Base-128 digits of an integer |X| <= 2^(7S-1): the lower S - 1 balanced in [-63, 64], the
-// top one the remaining quotient (|d_1| <= 64), so X = sum_s d_s 128^(S-s) exactly.
-template <int S>
-__device__ __forceinline__ void digits(long long X, int8_t* d) {
-#pragma unroll
-  for (int s = S - 1; s >= 1; --s) {
-    int r = (int)(X & 127);
-    r -= (r > 64) ? 128 : 0;
-    d[s] = (int8_t)r;
-    X = (X - r) >> 7;
-  }
-  d[0] = (int8_t)X;
-}
-
-// cut x (|x| < 1 after scaling) into S int8 slices: X = rint(x 2^(7S-1)) (one rounding, to
-// nearest even) split into digits, so x = 2 sum_s d_s 2^-7s + O(2^-7S) with every |d_s| <= 64
-// and an unbiased residual.  Integer arithmetic after one conversion (a chain of FP64
-// roundings per slice made the slicing pass compute-bound).
-template <int S>
-__device__ __forceinline__ void cut(double x, int8_t* d) {
-  digits<S>(__double2ll_rn(x * (double)(1LL << (7 * S - 1))), d);
-}
-
 // drain `NC` int32 columns (a multiple of 8, at most 32) starting at taddr into acc * scale
 template <int NC>
 __device__ __forceinline__ void drain_cols(uint32_t taddr, double* acc, double scale) {
@@ -228,36 +205,6 @@ __device__ __forceinline__ void drain_cols(uint32_t taddr, double* acc, double s
     // exact int32 -> double: the bits (0x43380000, r + 2^31) encode 2^52 + 2^51 + r + 2^31
     const double x = __hiloint2double(0x43380000, r[i] ^ (int)0x80000000) - 6755401588539392.0;
     acc[i] = fma(x, scale, acc[i]);
-  }
-}
-
-// Write x (a value of the target operand, |x| < 2^e) as S int8 slices at K index k of target
-// row (A planes) or complex column (B planes) `tr` of target batch `tb`.  X = rint(x 2^(7S-1-e))
-// (|X| <= 2^(7S-1)) is split into base-128 digits, the lower S - 1 balanced in [-63, 64] and the
-// top one the remaining quotient (|d_1| <= 64), by exact integer arithmetic, so that
-// x = 2^(e+1) sum_s d_s 2^-7s up to the rounding of X (|error| <= 2^(e-7S)).
-template <int S>
-__device__ __forceinline__ void emit_slices(double2 v, int e, const SplitEmit& em, long tb, int tr, long k) {
-  const double f = scale_pow2(7 * S - 1 - e);
-  int8_t dr[S], di[S];
-  digits<S>(__double2ll_rn(v.x * f), dr);
-  digits<S>(__double2ll_rn(v.y * f), di);
-  const long kb = k >> 5;
-  const int off = 2 * (int)(k & 31);
-  if (em.side == 0) {
-#pragma unroll
-    for (int s = 0; s < S; ++s) {
-      int8_t* o = em.planes + ((((tb * S + s) * em.nkb + kb) * em.rows + tr) << 6) + off;
-      *(char2*)o = make_char2(dr[s], di[s]);
-    }
-  } else {
-    // B' rows 2c: (re, -im); 2c + 1: (im, re)
-#pragma unroll
-    for (int s = 0; s < S; ++s) {
-      int8_t* o = em.planes + ((((tb * S + s) * em.nkb + kb) * (2L * em.rows) + 2L * tr) << 6) + off;
-      *(char2*)o = make_char2(dr[s], (int8_t)(-di[s]));
-      *(char2*)(o + 64) = make_char2(di[s], dr[s]);
-    }
   }
 }
 
@@ -284,8 +231,6 @@ struct I8Args {
   int nbuf;  // accumulator sets in TMEM (1 or 2)
   int a_shared, b_shared;  // operand identical for every batch: sliced once, planes / exponents of batch 0
   int* err;
-  SplitEmit em;            // em.on: the epilogue writes the product as int8 slices of another split
-                           // GEMM's operand instead of writing C
   SplitRowMax mx;          // mx.on: the epilogue also records the row maxima of C
   long long wait_cycles;   // limit of every barrier wait (WAIT_CYCLES; shorter in the time-out test)
   int skip_arrive;         // time-out test: CTA 0's first epilogue warp never releases the first
@@ -318,13 +263,11 @@ __device__ __forceinline__ Unit unit_of(const I8Args& p, long u, int BN) {
 // overwrites it, and with `reuse` it first waits until the epilogue has drained that
 // diagonal); LAST: the last K block (a commit per diagonal tells the epilogue that the
 // diagonal is complete).  Descriptor offsets are compile-time constants.
-// (A runtime loop: these first / last K blocks of a segment are few per tile, and unrolled
-// copies of them made the kernel larger than the instruction cache.)
 template <int S, int BN, bool FIRST, bool LAST>
 __device__ __forceinline__ bool issue_kblock(uint32_t tacc0, uint64_t da, uint64_t db, uint32_t idesc, uint32_t leader,
                                              bool reuse, uint64_t* acce, uint64_t* accf, uint32_t par_e,
                                              volatile int* err, long long limit) {
-#pragma unroll 1
+#pragma unroll
   for (int d = 2; d <= S + 1; ++d) {
     if (FIRST && reuse) {
       if (!__all_sync(0xffffffffu, mbar_wait(&acce[d - 2], par_e, err, 2, limit))) return false;
@@ -332,7 +275,7 @@ __device__ __forceinline__ bool issue_kblock(uint32_t tacc0, uint64_t da, uint64
     }
     const uint32_t tacc = tacc0 + (uint32_t)((d - 2) * BN);
     const int s_lo = d - S > 1 ? d - S : 1, s_hi = d - 1 < S ? d - 1 : S;
-#pragma unroll 1
+#pragma unroll
     for (int s = s_lo; s <= s_hi; ++s) {
       const int t = d - s;
       const uint64_t a = da + (uint64_t)(((s - 1) * BM * KB) >> 4);
@@ -570,33 +513,6 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       const double sa = pow2i(ea);  // row factor; x = 2 sum d_s 2^-7s per operand gives the + 2
       double2* crow = p.C + b0 * p.c_b0 + b1 * p.c_b1 + b2 * p.c_b2 + (mok ? p.c_m(m) : 0);
       double2* wrow = p.work + (w.split * p.batch + w.batch) * (long)p.N * p.M + m;
-      if (p.em.on) {
-        // the product as slices of the target operand: (m, n, batch) -> target (batch, row or
-        // column, K index); the target's exponent comes from a bound computed beforehand
-        const SplitEmit& em = p.em;
-        const int mq = m / em.div_m, mr = m - mq * em.div_m;
-        int eq = nbase / em.div_n, er = nbase - eq * em.div_n;
-        const long kbase = w.batch * em.k_b + (long)mr * em.k_m;
-#pragma unroll
-        for (int c = 0; c < HC / 2; ++c) {
-          const int eb = __shfl_sync(0xffffffffu, eb_lane, c);
-          if (mok && nbase + c < p.N) {
-            const double sb = pow2i(eb + 2);
-            const double2 v = make_double2(acc[2 * c] * sa * sb, acc[2 * c + 1] * sa * sb);
-            const long tb = em.batch_from_n ? eq : mq;
-            const int tr = em.batch_from_n ? mq : eq;
-            emit_slices<S>(v, em.ex[tb * em.ex_ld + tr], em, tb, tr, kbase + (long)er * em.k_n);
-          }
-          if (++er == em.div_n) {
-            er = 0;
-            ++eq;
-          }
-        }
-        continue;
-      }
-      // column offset c_n(n) stepped through the tile: (nq, nr) = divmod(n, split)
-      const int csp = p.c_n.split > 0 ? p.c_n.split : 1 << 30;
-      int nq = nbase / csp, nr = nbase - nq * csp;
       if (p.mx.on) {
         // row maxima for the next GEMM (kept out of the store loop below, whose code stays
         // compact): a run of columns with the same column key is reduced per thread, then over
@@ -633,6 +549,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
         if (xr != 0) xflush(xq);
       }
+      // column offset c_n(n) stepped through the tile: (nq, nr) = divmod(n, split)
+      const int csp = p.c_n.split > 0 ? p.c_n.split : 1 << 30;
+      int nq = nbase / csp, nr = nbase - nq * csp;
 #pragma unroll
       for (int c = 0; c < HC / 2; ++c) {
         const int eb = __shfl_sync(0xffffffffu, eb_lane, c);
@@ -737,6 +656,26 @@ __global__ void row_exponent_rc_kernel(OpView v, int rows_pad, int* out, long nb
   out[gt] = mx > 0.0 ? ilogb(mx) + 1 : 0;
 }
 
+
+// cut x (|x| < 1 after scaling) into S int8 slices by rounding to nearest:
+// d_1 = rint(64 x), r_1 = 64 x - d_1 in [-1/2, 1/2]; d_s = rint(128 r_{s-1}), ...
+// so x = 2 sum_s d_s 2^-7s + O(2^-7S), every |d_s| <= 64 and the residual is unbiased.
+// rint is done by adding 2^52 + 2^51 (the sum is rounded to an integer, round-to-nearest-
+// even like rint, and its low word holds that integer in two's complement); every step is
+// exact in FP64 and uses only the add / fma pipes (measured faster than one rounding to int64
+// followed by integer digit extraction).
+template <int S>
+__device__ __forceinline__ void cut(double x, int8_t* d) {
+  const double RND = 6755399441055744.0;  // 2^52 + 2^51
+  x *= 64.0;
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const double y = x + RND;
+    d[s] = (int8_t)__double2loint(y);
+    const double t = y - RND;
+    x = (x - t) * 128.0;
+  }
+}
 
 // x * 2^-e, exact while the result is a normal number (ldexp outside the directly encodable range)
 __device__ __forceinline__ double scale_neg(double x, int e) {
@@ -985,7 +924,7 @@ Geometry geometry(const ZgemmDesc& d, int S) {
 
 // the persistent INT8 GEMM on operand planes (a8 / b8 of batch_a / batch_b batches)
 int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const int8_t* a8, const int8_t* b8,
-               const int* ea, const int* eb, bool a_shared, bool b_shared, const SplitEmit* em, cudaStream_t st,
+               const int* ea, const int* eb, bool a_shared, bool b_shared, cudaStream_t st,
                const SplitRowMax* mx = nullptr) {
   int* err = e->err.p;
   if (!err) {
@@ -1020,7 +959,6 @@ int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const
   a.alpha = d.alpha;
   a.beta = d.beta;
   a.err = err;
-  if (em) a.em = *em;
   if (mx) a.mx = *mx;
   a.wait_cycles = WAIT_CYCLES;
   a.skip_arrive = 0;
@@ -1042,9 +980,9 @@ int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const
   const size_t smem = a.stages * stage_bytes + 1024 + 512;  // + alignment + barriers and TMEM slot
   const long base = (long)a.tiles_m * a.tiles_n * g.batch;
   // split-K so that the units fill whole waves of persistent CTAs (each split keeps >= 8 K
-  // blocks); an emitting epilogue needs whole reductions (no split-K)
+  // blocks); the row-max epilogue needs whole reductions (no split-K)
   int splits = 1;
-  if (!a.em.on && !a.mx.on) {
+  if (!a.mx.on) {
     const int smax = (int)std::max<long>(1, std::min<long>(g.nkb / 8, 64));
     double best = 0.0;
     for (int sp = 1; sp <= smax; ++sp) {
@@ -1095,8 +1033,8 @@ int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const
 }
 
 // exponents and slices of both operands into the engine's planes, then the GEMM
-int sliced_gemm(SplitGemm* e, const ZgemmDesc& d, int S, const SplitEmit* em, cudaStream_t st,
-                const SplitRowMax* mx = nullptr, const int* ea_given = nullptr, const int* eb_given = nullptr) {
+int sliced_gemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st, const SplitRowMax* mx = nullptr,
+                const int* ea_given = nullptr, const int* eb_given = nullptr) {
   if (d.M <= 0 || d.N <= 0) return 0;
   const Geometry g = geometry(d, S);
   // an operand with zero batch strides is the same matrix for every batch: slice it once
@@ -1134,7 +1072,7 @@ int sliced_gemm(SplitGemm* e, const ZgemmDesc& d, int S, const SplitEmit* em, cu
     ++launches;
   }
   launch_slices(S, va, vb, g.rows_a_pad, g.ncol_pad, g.nkb, ea, eb, a8, b8, batch_a, batch_b, st);
-  return launches + run_planes(e, d, S, g, a8, b8, ea, eb, a_shared, b_shared, em, st, mx);
+  return launches + run_planes(e, d, S, g, a8, b8, ea, eb, a_shared, b_shared, st, mx);
 }
 
 }  // namespace
@@ -1152,36 +1090,21 @@ SplitPlanes split_planes_for(const ZgemmDesc& d, int S) {
   return p;
 }
 
-int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) { return sliced_gemm(e, d, S, nullptr, st); }
-
-int split_zgemm_emit(SplitGemm* e, const ZgemmDesc& d, int S, const SplitEmit& em, cudaStream_t st) {
-  if (!em.on || !em.planes || !em.ex || em.div_m < 1 || em.div_n < 1 || em.nkb < 1 || em.rows < 1)
-    throw Error(GG_ERR_ARG, "split emit: incomplete target description");
-  if (d.alpha.x != 1.0 || d.alpha.y != 0.0 || d.beta.x != 0.0 || d.beta.y != 0.0)
-    throw Error(GG_ERR_ARG, "split emit: alpha must be 1 and beta 0");
-  return sliced_gemm(e, d, S, &em, st);
-}
+int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st) { return sliced_gemm(e, d, S, st); }
 
 int split_zgemm_rowmax(SplitGemm* e, const ZgemmDesc& d, int S, const SplitRowMax& mx, cudaStream_t st) {
   if (!mx.on || !mx.ex || mx.div_m < 1 || mx.div_n < 1)
     throw Error(GG_ERR_ARG, "split row max: incomplete target description");
   if (d.alpha.x != 1.0 || d.alpha.y != 0.0 || d.beta.x != 0.0 || d.beta.y != 0.0)
     throw Error(GG_ERR_ARG, "split row max: alpha must be 1 and beta 0");
-  return sliced_gemm(e, d, S, nullptr, st, &mx);
+  return sliced_gemm(e, d, S, st, &mx);
 }
 
 int split_zgemm_exps(SplitGemm* e, const ZgemmDesc& d, int S, const int* ea, const int* eb, cudaStream_t st,
                      const SplitRowMax* mx) {
   if (mx && (d.alpha.x != 1.0 || d.alpha.y != 0.0 || d.beta.x != 0.0 || d.beta.y != 0.0))
     throw Error(GG_ERR_ARG, "split row max: alpha must be 1 and beta 0");
-  return sliced_gemm(e, d, S, nullptr, st, mx, ea, eb);
-}
-
-int split_zgemm_planes(SplitGemm* e, const ZgemmDesc& d, int S, const int8_t* a8, const int8_t* b8, const int* ea,
-                       const int* eb, cudaStream_t st) {
-  if (d.M <= 0 || d.N <= 0) return 0;
-  const Geometry g = geometry(d, S);
-  return run_planes(e, d, S, g, a8, b8, ea, eb, false, false, nullptr, st);
+  return sliced_gemm(e, d, S, st, mx, ea, eb);
 }
 
 void split_check(SplitGemm* e, cudaStream_t st) {

@@ -6,26 +6,6 @@
 
 namespace gg {
 
-// Epilogue that writes a build GEMM's product C(m, n) of batch b directly as int8 slices of
-// another split GEMM's operand (its K-blocked planes), skipping the FP64 product and the
-// exponent / slicing passes over it.  With m = mq div_m + mr and n = nq div_n + nr, the element
-// goes to target batch tb and target row (A planes) or complex column (B planes) tr, with
-// (tb, tr) = (nq, mq) when batch_from_n, else (mq, nq), at target K index
-// b k_b + mr k_m + nr k_n.  Its scale is the target's exponent ex[tb * ex_ld + tr], which must
-// bound the target row / column: every |Re|, |Im| < 2^ex.  alpha = 1, beta = 0 only.
-struct SplitEmit {
-  int on = 0;
-  int side = 0;          // 0: A planes [tb][S][nkb][rows][64 B]; 1: B planes [tb][S][nkb][2 rows][64 B]
-  int div_m = 1, div_n = 1;
-  int batch_from_n = 0;
-  long k_b = 0, k_m = 0, k_n = 0;
-  long nkb = 0;          // K blocks of the target planes
-  long rows = 0;         // A: padded rows of a target plane; B: padded complex columns
-  long ex_ld = 0;
-  const int* ex = nullptr;
-  int8_t* planes = nullptr;
-};
-
 // Epilogue that also records the exact row maxima of the product for the next split GEMM: with
 // m = mq div_m + mr and n = nq div_n + nr, |Re C|, |Im C| of (m, n) of batch b count towards
 // entry ex[b * s_b + mq * s_mq + mr * s_mr + nq * s_nq], which receives (by atomicMax over all
@@ -53,8 +33,6 @@ struct SplitGemm;
 SplitGemm* split_engine(gg_context* c);
 // Same contract as zgemm() for descriptors with KB >= 1; FP64 in, FP64 out.
 int split_zgemm(SplitGemm* e, const ZgemmDesc& d, int slices, cudaStream_t st);
-// Same, with the epilogue writing slices of another operand (em.on = 1; no C written).
-int split_zgemm_emit(SplitGemm* e, const ZgemmDesc& d, int slices, const SplitEmit& em, cudaStream_t st);
 // Same as split_zgemm, recording the row maxima of C as described by mx (alpha = 1, beta = 0).
 int split_zgemm_rowmax(SplitGemm* e, const ZgemmDesc& d, int slices, const SplitRowMax& mx, cudaStream_t st);
 // split_zgemm with operand exponents given (ea [batch][rows_a_pad], eb [batch][N], as
@@ -62,10 +40,6 @@ int split_zgemm_rowmax(SplitGemm* e, const ZgemmDesc& d, int slices, const Split
 // recording the row maxima of its own product (mx may be NULL).
 int split_zgemm_exps(SplitGemm* e, const ZgemmDesc& d, int slices, const int* ea, const int* eb, cudaStream_t st,
                      const SplitRowMax* mx = nullptr);
-// The GEMM of descriptor d (d.A / d.B unused) on operands already in planes of geometry
-// split_planes_for(d, slices), with exponents ea [batch][rows_a_pad] and eb [batch][N].
-int split_zgemm_planes(SplitGemm* e, const ZgemmDesc& d, int slices, const int8_t* a8, const int8_t* b8,
-                       const int* ea, const int* eb, cudaStream_t st);
 void split_release(SplitGemm* e);
 // Make the next launch of this engine run the time-out test (short wait limit, one accumulator
 // release withheld by CTA 0), so that its failure path is exercised without any fault.
