@@ -246,6 +246,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="eager builds instead of graph replays")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 build of the same system")
+    ap.add_argument("--no-autotune", action="store_true", help="tile widths and split-K by the rules only")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -291,6 +292,8 @@ def main():
     # graph mode: the first warm-up build runs eagerly and is captured; the later builds replay
     # the captured graph (one launch per build).  No profiling events inside the timed region.
     ctx.set_graph(not args.no_graph)
+    if args.precision == "split" and not args.no_autotune:
+        ctx.set_autotune(True)  # the first warm-up build times the tile candidates of every shape
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize(dev)
@@ -414,6 +417,7 @@ def main():
         "gpu_launches": launches_per_build * args.steps,
         "timed_region": ("graph replays, no profiling events" if not args.no_graph else "eager builds, no profiling "
                          "events") + "; phases_s and roofline from one profiled eager build after it",
+        "autotune": ctx.autotune_report().splitlines() if args.precision == "split" and not args.no_autotune else None,
         "clocks": clk.summary(),
         "e2e": {"value": (1.0 / statistics.mean(e2e_t)) if e2e_t else None, "unit": "builds/s",
                 "h2d_bytes_per_step": gbytes, "d2h_bytes_per_step": gbytes},

@@ -610,6 +610,15 @@ int gg_symmetry_unfold(gg_context* c, const double* X_ibz, int64_t nmat, double*
   });
 }
 
+int gg_set_autotune(gg_context* c, int enable) {
+  return guarded(c, [&] {
+    split_set_autotune(split_engine(c), enable != 0);
+    c->drop_graph();  // a captured graph holds the launch configurations of the old setting
+  });
+}
+
+const char* gg_autotune_report(const gg_context* c) { return c ? split_autotune_report(c->split) : ""; }
+
 int gg_arm_split_timeout_test(gg_context* c) {
   return guarded(c, [&] { split_arm_timeout_test(split_engine(c)); });
 }

@@ -31,9 +31,12 @@
 #include <cuda.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <string>
 
 #include "kernels.cuh"
 
@@ -45,6 +48,14 @@ struct SplitGemm {
   DevBuf<double2> work;
   int err_host = 0;
   bool timeout_test = false;  // the next launch runs the time-out test (one-shot)
+  // tile autotuner: per GEMM shape the (tile width, split-K factor) that measured fastest
+  bool autotune = false;
+  struct Choice {
+    int BN, splits;
+    double ms;
+  };
+  std::map<std::array<long, 8>, Choice> tuned;
+  std::string report;
 };
 
 namespace {
@@ -870,6 +881,16 @@ void split_release(SplitGemm* e) { delete e; }
 
 void split_arm_timeout_test(SplitGemm* e) { e->timeout_test = true; }
 
+void split_set_autotune(SplitGemm* e, bool on) {
+  e->autotune = on;
+  if (!on) {
+    e->tuned.clear();
+    e->report.clear();
+  }
+}
+
+const char* split_autotune_report(const SplitGemm* e) { return e ? e->report.c_str() : ""; }
+
 void split_buffers(const SplitGemm* e, std::vector<const void*>& out) {
   if (!e) {
     out.push_back(nullptr);
@@ -884,9 +905,18 @@ namespace {
 struct Geometry {
   int BN, nbuf, rows_a_pad, rows_b_pad, ncol_pad, nkb, kcb;
   long batch, Ktot, kp;
+  int rows_b_plane;  // height of a B plane (>= rows_b_pad when planes are shared by several widths)
 };
 
-Geometry geometry(const ZgemmDesc& d, int S) {
+// tile widths of the INT8 kernels instantiated for S slices (accumulators of S x BN columns fit TMEM)
+std::vector<int> widths(int S) {
+  if (S == 5) return {96, 80, 64};
+  if (S == 6) return {80, 64};
+  if (S <= 4) return {128};
+  return {64};
+}
+
+Geometry geometry(const ZgemmDesc& d, int S, int force_bn = 0) {
   if (S < 2 || S > 8) throw Error(GG_ERR_ARG, "split: slices must be in [2, 8]");
   Geometry g;
   // nbuf accumulator sets of S diagonals x BN columns must fit the 512 TMEM columns;
@@ -913,8 +943,10 @@ Geometry geometry(const ZgemmDesc& d, int S) {
     throw Error(GG_ERR_ARG, "split: operand dimensions too large for one launch");
   g.kp = ((2 * g.Ktot + KB - 1) / KB) * KB;
   g.rows_a_pad = ((d.M + BM - 1) / BM) * BM;
+  if (force_bn) g.BN = force_bn;
   g.rows_b_pad = ((2 * d.N + g.BN - 1) / g.BN) * g.BN;  // B' rows (2 per complex column), whole tiles
   g.ncol_pad = g.rows_b_pad / 2;                        // complex columns incl. padding
+  g.rows_b_plane = g.rows_b_pad;
   // exact int32 chunk: S * Kchunk * 64^2 < 2^31 (slices are rounded, |d| <= 64)
   const long kchunk = std::max<long>(KB, ((2147483647L / (4096L * S)) / KB) * KB);
   g.kcb = (int)(kchunk / KB);
@@ -925,7 +957,7 @@ Geometry geometry(const ZgemmDesc& d, int S) {
 // the persistent INT8 GEMM on operand planes (a8 / b8 of batch_a / batch_b batches)
 int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const int8_t* a8, const int8_t* b8,
                const int* ea, const int* eb, bool a_shared, bool b_shared, cudaStream_t st,
-               const SplitRowMax* mx = nullptr) {
+               const SplitRowMax* mx = nullptr, int force_splits = 0) {
   int* err = e->err.p;
   if (!err) {
     err = e->err.ensure(1);
@@ -933,7 +965,7 @@ int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const
   }
   const long batch_a = a_shared ? 1 : g.batch, batch_b = b_shared ? 1 : g.batch;
   const CUtensorMap ta = make_map(a8, g.rows_a_pad, batch_a * S * g.nkb, BM);
-  const CUtensorMap tb = make_map(b8, g.rows_b_pad, batch_b * S * g.nkb, g.BN);
+  const CUtensorMap tb = make_map(b8, g.rows_b_plane, batch_b * S * g.nkb, g.BN);
 
   I8Args a{};
   a.S = S;
@@ -982,7 +1014,9 @@ int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const
   // split-K so that the units fill whole waves of persistent CTAs (each split keeps >= 8 K
   // blocks); the row-max epilogue needs whole reductions (no split-K)
   int splits = 1;
-  if (!a.mx.on) {
+  if (force_splits > 0) {
+    splits = a.mx.on ? 1 : force_splits;
+  } else if (!a.mx.on) {
     const int smax = (int)std::max<long>(1, std::min<long>(g.nkb / 8, 64));
     double best = 0.0;
     for (int sp = 1; sp <= smax; ++sp) {
@@ -1036,13 +1070,37 @@ int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const
 int sliced_gemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st, const SplitRowMax* mx = nullptr,
                 const int* ea_given = nullptr, const int* eb_given = nullptr) {
   if (d.M <= 0 || d.N <= 0) return 0;
-  const Geometry g = geometry(d, S);
+  Geometry g = geometry(d, S);
   // an operand with zero batch strides is the same matrix for every batch: slice it once
   const bool a_shared = g.batch > 1 && d.a_b0 == 0 && d.a_b1 == 0 && d.a_b2 == 0;
   const bool b_shared = g.batch > 1 && d.b_b0 == 0 && d.b_b1 == 0 && d.b_b2 == 0;
   const long batch_a = a_shared ? 1 : g.batch, batch_b = b_shared ? 1 : g.batch;
+  // autotuner: a shape seen before runs with its measured best (tile width, split-K); a new
+  // shape is timed for every candidate when this call may run more than once (it overwrites C,
+  // beta = 0) and is not being captured into a graph
+  const std::array<long, 8> key{S, d.M, d.N, g.Ktot, g.batch, (a_shared ? 1 : 0) + (b_shared ? 2 : 0),
+                                mx ? 1 : 0, g.nkb};
+  int force_splits = 0;
+  bool tune = false;
+  std::vector<int> cand_bn;
+  if (e->autotune) {
+    auto it = e->tuned.find(key);
+    if (it != e->tuned.end()) {
+      g = geometry(d, S, it->second.BN);
+      force_splits = it->second.splits;
+    } else {
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      GG_CUDA(cudaStreamIsCapturing(st, &cs));
+      tune = cs == cudaStreamCaptureStatusNone && d.beta.x == 0.0 && d.beta.y == 0.0;
+      if (tune) {
+        cand_bn = widths(S);
+        for (int bn : cand_bn) g.rows_b_plane = std::max(g.rows_b_plane, geometry(d, S, bn).rows_b_pad);
+        g.ncol_pad = g.rows_b_plane / 2;  // slice B once, tall enough for every candidate width
+      }
+    }
+  }
   int8_t* a8 = e->a8.ensure((size_t)batch_a * S * g.rows_a_pad * g.kp);
-  int8_t* b8 = e->b8.ensure((size_t)batch_b * S * g.rows_b_pad * g.kp);
+  int8_t* b8 = e->b8.ensure((size_t)batch_b * S * g.rows_b_plane * g.kp);
   int* ea = e->ea.ensure((size_t)batch_a * g.rows_a_pad);
   int* eb = e->eb.ensure((size_t)batch_b * d.N);
   OpView va{d.A, d.a_m, d.a_kb, d.a_k, d.KB, d.K, d.M, d.nb0, d.nb1, d.a_b0, d.a_b1, d.a_b2, d.conjA};
@@ -1072,7 +1130,59 @@ int sliced_gemm(SplitGemm* e, const ZgemmDesc& d, int S, cudaStream_t st, const 
     ++launches;
   }
   launch_slices(S, va, vb, g.rows_a_pad, g.ncol_pad, g.nkb, ea, eb, a8, b8, batch_a, batch_b, st);
-  return launches + run_planes(e, d, S, g, a8, b8, ea, eb, a_shared, b_shared, st, mx);
+  if (!tune) return launches + run_planes(e, d, S, g, a8, b8, ea, eb, a_shared, b_shared, st, mx, force_splits);
+  // time every (width, split-K) candidate on the sliced planes; the rule's split-K factor, one
+  // and twice the rule's bracket the split-K choice
+  cudaEvent_t t0, t1;
+  GG_CUDA(cudaEventCreate(&t0));
+  GG_CUDA(cudaEventCreate(&t1));
+  SplitGemm::Choice best{g.BN, 0, 1e30};
+  for (int bn : cand_bn) {
+    Geometry gc = geometry(d, S, bn);
+    gc.rows_b_plane = g.rows_b_plane;
+    gc.ncol_pad = g.ncol_pad;
+    const long base = (long)(gc.rows_a_pad / BM) * (gc.rows_b_pad / bn) * gc.batch;
+    int rule = 1;
+    {
+      const int smax = (int)std::max<long>(1, std::min<long>(gc.nkb / 8, 64));
+      double b = 0.0;
+      for (int sp = 1; sp <= smax; ++sp) {
+        const long units = base * sp, waves = (units + sms() - 1) / sms();
+        const double eff = (double)units / (double)(waves * sms());
+        if (eff > b + 0.05) {
+          b = eff;
+          rule = sp;
+        }
+        if (units >= 4L * sms()) break;
+      }
+    }
+    const int smax = mx ? 1 : (int)std::max<long>(1, std::min<long>(gc.nkb / 8, 64));
+    std::vector<int> sps{rule, 1, std::min(2 * rule, smax)};
+    std::sort(sps.begin(), sps.end());
+    sps.erase(std::unique(sps.begin(), sps.end()), sps.end());
+    for (int sp : sps) {
+      if (mx && sp != 1) continue;
+      GG_CUDA(cudaEventRecord(t0, st));
+      launches += run_planes(e, d, S, gc, a8, b8, ea, eb, a_shared, b_shared, st, mx, sp);
+      GG_CUDA(cudaEventRecord(t1, st));
+      GG_CUDA(cudaEventSynchronize(t1));
+      float ms = 0.f;
+      GG_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+      if (ms < best.ms) best = {bn, sp, ms};
+    }
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  e->tuned[key] = best;
+  char line[200];
+  std::snprintf(line, sizeof(line), "S %ld M %ld N %ld K %ld batch %ld: BN %d split-K %d (%.3f ms)\n", key[0], key[1],
+                key[2], key[3], key[4], best.BN, best.splits, best.ms);
+  e->report += line;
+  // the result of this call comes from the chosen configuration, as every later call's will
+  Geometry gb = geometry(d, S, best.BN);
+  gb.rows_b_plane = g.rows_b_plane;
+  gb.ncol_pad = g.ncol_pad;
+  return launches + run_planes(e, d, S, gb, a8, b8, ea, eb, a_shared, b_shared, st, mx, best.splits);
 }
 
 }  // namespace

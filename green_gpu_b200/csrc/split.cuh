@@ -44,6 +44,12 @@ void split_release(SplitGemm* e);
 // Make the next launch of this engine run the time-out test (short wait limit, one accumulator
 // release withheld by CTA 0), so that its failure path is exercised without any fault.
 void split_arm_timeout_test(SplitGemm* e);
+// Tile autotuner of the INT8 engine (per engine): the first call of every GEMM shape that
+// overwrites its output and is not being captured times each candidate tile width and split-K
+// factor with CUDA events and keeps the fastest for every later call of that shape.
+void split_set_autotune(SplitGemm* e, bool on);
+// One line per tuned shape: "S M N K batch: BN b split-K s (t ms)".
+const char* split_autotune_report(const SplitGemm* e);
 // Device addresses of the engine's work buffers (appended to `out`): a graph that captured
 // split GEMMs stays valid only while none of them was reallocated.
 void split_buffers(const SplitGemm* e, std::vector<const void*>& out);

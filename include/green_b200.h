@@ -261,6 +261,18 @@ int gg_chemical_potential(int32_t ns, int32_t ink, int32_t n, const double* weig
  * context-free, allocates nothing.  Used for admission by memory footprint. */
 int gg_estimate_bytes(const gg_shape* shape, int64_t num_kpair_stored, int64_t* bytes);
 
+/* Tile autotuner of the split-precision INT8 engine (no counterpart in the reference, whose
+ * GEMMs are cuBLAS calls).  With it enabled, the first call of every distinct GEMM shape on this
+ * context that overwrites its output (beta = 0) and is not being captured into a CUDA graph is
+ * run once for every candidate tile width (96 / 80 / 64 B' rows at 5 slices) and split-K factor
+ * (the wave-filling rule's, one, twice the rule's), timed with CUDA events on the call's stream;
+ * that call's result and every later call of the shape use the fastest.  Tile width does not
+ * change any element's arithmetic; split-K changes only the FP64 summation order of the partial
+ * sums.  gg_autotune_report returns one line per tuned shape (valid until the next call on the
+ * context).  Disabling clears the choices. */
+int gg_set_autotune(gg_context* ctx, int enable);
+const char* gg_autotune_report(const gg_context* ctx);
+
 /* Test hook of the split engine's time-out path (no counterpart in the reference, whose device
  * lock spins without a limit: src/cuda_common.cu:225-231).  The next split-precision GEMM on
  * this context runs with a 0.1 s limit on every barrier wait, and one epilogue warp of CTA 0

@@ -81,3 +81,28 @@ def test_fp64_zgemm_tile_runs_match_numpy(ctx, M, N):
     A = rng.standard_normal((M, K)) + 1j * rng.standard_normal((M, K))
     B = rng.standard_normal((K, N)) + 1j * rng.standard_normal((K, N))
     assert rel(ctx.zgemm(A, B), A @ B) < 1e-14
+
+
+def test_autotuner_picks_a_configuration_per_shape_and_keeps_results():
+    # the tuned configuration changes only the FP64 order of split-K partial sums, so a tuned
+    # GW build equals the untuned one to rounding (1e-13) and the oracle to the split tolerance
+    s = synth.make_system(mesh=(2, 2, 1), nao=8, NQ=24, ns=1, beta=10.0, lam=100.0, nts=24, nw_b=21, seed=9,
+                          symmetry="none")
+    plain = native.context_for(s)
+    ref = plain.gw_sigma(s.G_tskij, precision=native.PREC_SPLIT)
+    c = native.context_for(s)
+    c.set_autotune(True)
+    first = c.gw_sigma(s.G_tskij, precision=native.PREC_SPLIT)   # tunes every shape
+    report = c.autotune_report().splitlines()
+    assert report and all("BN" in line and "split-K" in line for line in report)
+    second = c.gw_sigma(s.G_tskij, precision=native.PREC_SPLIT)  # uses the tuned choices
+    assert np.array_equal(first, second)
+    assert rel(first, ref) < 1e-13
+    assert rel(first, ogw.gw_build(s)) < 1e-8
+    assert c.autotune_report().splitlines() == report           # nothing re-tuned
+    c.set_graph(True)                                             # tuned shapes also replay in a graph
+    g1 = c.gw_sigma(s.G_tskij, precision=native.PREC_SPLIT)
+    g2 = c.gw_sigma(s.G_tskij, precision=native.PREC_SPLIT)
+    assert np.array_equal(g1, first) and np.array_equal(g2, first)
+    plain.close()
+    c.close()
