@@ -62,7 +62,8 @@ namespace {
 
 constexpr int BM = 128;        // UMMA M (rows of A per tile)
 constexpr int KB = 64;         // K bytes per pipeline stage (one 64-byte swizzle row)
-constexpr int NTHREADS = 320;  // 10 warps
+constexpr int EPI_WARPS = 16;  // epilogue warps: 4 TMEM lane quadrants x 4 column quarters
+constexpr int NTHREADS = 32 * (2 + EPI_WARPS);  // + the TMA warp and the MMA warp
 constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s at B200 clocks
 
 // ------------------------------------------------------------------ PTX helpers
@@ -185,10 +186,13 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, int* r) {
                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
                : "r"(taddr));
 }
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-__device__ __forceinline__ void reg_fence8(int* r) {
-  asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]));
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, int* r) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr));
 }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void reg_fence4(int* r) { asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3])); }
 
 // 2^e as a double, e clamped to the normal range (operand exponents come from ilogb of
 // finite data, so a row factor times a column factor covers every representable result;
@@ -201,16 +205,18 @@ __device__ __forceinline__ double pow2i(int e) {
 // 2^e for e in the normal range (exact)
 __device__ __forceinline__ double scale_pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
 
-// drain `NC` int32 columns (a multiple of 8, at most 32) starting at taddr into acc * scale
+// drain `NC` int32 columns (a multiple of 4, at most 32) starting at taddr into acc * scale
 template <int NC>
 __device__ __forceinline__ void drain_cols(uint32_t taddr, double* acc, double scale) {
+  static_assert(NC % 4 == 0 && NC <= 32, "TMEM loads of 4, 8 or 16 columns");
   int r[32];
 #pragma unroll
   for (int j = 0; j < NC / 16; ++j) tmem_ld16(taddr + j * 16, r + j * 16);
-  if constexpr (NC % 16 == 8) tmem_ld8(taddr + (NC / 16) * 16, r + (NC / 16) * 16);
+  if constexpr (NC % 16 >= 8) tmem_ld8(taddr + (NC / 16) * 16, r + (NC / 16) * 16);
+  if constexpr (NC % 8 == 4) tmem_ld4(taddr + (NC / 8) * 8, r + (NC / 8) * 8);
   tmem_wait_ld();
 #pragma unroll
-  for (int j = 0; j < NC / 8; ++j) reg_fence8(r + j * 8);
+  for (int j = 0; j < NC / 4; ++j) reg_fence4(r + j * 4);
 #pragma unroll
   for (int i = 0; i < NC; ++i) {
     // exact int32 -> double: the bits (0x43380000, r + 2^31) encode 2^52 + 2^51 + r + 2^31
@@ -361,7 +367,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
     for (int b = 0; b < 2 * ND; ++b) {
       mbar_init(&accf[b], 1);
-      mbar_init(&acce[b], 8);
+      mbar_init(&acce[b], EPI_WARPS);
     }
     mbar_init(fin, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -466,10 +472,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       mbar_wait(fin, 0, err, 32, p.wait_cycles, false);
     }
   } else {
-    // ---------------- epilogue: 8 warps, lanes 32*(warp%4).., column half (warp-2)/4
+    // ---------------- epilogue: EPI_WARPS warps, lanes 32*(warp%4).. (the TMEM lane quadrant a
+    // warp may access), column part (warp-2)/4 of EPI_WARPS/4
     const int q = warp & 3, h = (warp - 2) >> 2;
     const int row = q * 32 + lane;
-    constexpr int HC = BN / 2;  // int32 columns per thread
+    constexpr int HC = BN / (EPI_WARPS / 4);  // int32 columns per thread
+    static_assert(HC % 4 == 0 && HC / 2 <= 32, "column part: a multiple of 4 int32 columns, at most 32 complex");
     double acc[HC];
     int buf = 0;
     uint32_t par = 0;
@@ -745,29 +753,30 @@ __global__ void slice_kernel(OpView v, int rows_pad, int ktiles, const int* ex, 
     }
   }
   __syncthreads();
-  // write: thread (ty -> row, tx -> kk)
+  // write: thread (ty -> row, tx -> kk).  Plane addresses are formed once per thread and
+  // stepped by the row and slice strides (the full index per store made this pass issue-bound).
+  const long plane = (BSIDE ? 2L : 1L) * rows_pad * KB;  // bytes of one K-block plane
+  const long sstride = (long)ktiles * plane;              // from slice s to s + 1
+  const int8_t* const obase = out + (b * S * ktiles + kt) * plane + 2 * tx;
+  const int* const exb = ex + b * (BSIDE ? v.R : rows_pad);
   for (int i = ty; i < 32; i += 8) {
     const int r = rt * 32 + i;
     if (r >= rows_pad) break;
     const double2 x = tile[i][tx];
-    const int e = (r < v.R) ? ex[b * (BSIDE ? v.R : rows_pad) + r] : 0;
+    const int e = (r < v.R) ? exb[r] : 0;
     int8_t dr[S], di[S];
     cut<S>(scale_neg(x.x, e), dr);
     cut<S>(scale_neg(x.y, e), di);
+    int8_t* o = const_cast<int8_t*>(obase) + (BSIDE ? 2L * r : (long)r) * KB;
     if (!BSIDE) {
 #pragma unroll
-      for (int s = 0; s < S; ++s) {
-        int8_t* o = out + ((((b * S + s) * ktiles + kt) * rows_pad + r) * KB + 2 * tx);
-        *(char2*)o = make_char2(dr[s], di[s]);
-      }
+      for (int s = 0; s < S; ++s, o += sstride) *(char2*)o = make_char2(dr[s], di[s]);
     } else {
       // B' rows 2r: (re, -im); 2r + 1: (im, re); rows_pad here counts complex columns
 #pragma unroll
-      for (int s = 0; s < S; ++s) {
-        int8_t* o0 = out + ((((b * S + s) * ktiles + kt) * (2L * rows_pad) + 2 * r) * KB + 2 * tx);
-        int8_t* o1 = o0 + KB;
-        *(char2*)o0 = make_char2(dr[s], (int8_t)(-di[s]));
-        *(char2*)o1 = make_char2(di[s], dr[s]);
+      for (int s = 0; s < S; ++s, o += sstride) {
+        *(char2*)o = make_char2(dr[s], (int8_t)(-di[s]));
+        *(char2*)(o + KB) = make_char2(di[s], dr[s]);
       }
     }
   }
