@@ -919,7 +919,7 @@ struct Geometry {
 
 // tile widths of the INT8 kernels instantiated for S slices (accumulators of S x BN columns fit TMEM)
 std::vector<int> widths(int S) {
-  if (S == 5) return {96, 80, 64};
+  if (S == 5) return {96, 80, 64, 48};
   if (S == 6) return {80, 64};
   if (S <= 4) return {128};
   return {64};
@@ -930,15 +930,14 @@ Geometry geometry(const ZgemmDesc& d, int S, int force_bn = 0) {
   Geometry g;
   // nbuf accumulator sets of S diagonals x BN columns must fit the 512 TMEM columns;
   // BN <= 128 keeps the FP64 drain registers (BN / 2 per thread) in budget
-  g.nbuf = S <= 2 ? 2 : 1;
   // tile width: the widest one whose accumulators fit TMEM, or a narrower one that pads the
   // 2N rows of B' less (2N = 800: 80 divides it, 96 pads it to 864)
   g.BN = S <= 4 ? 128 : S == 5 ? 96 : S == 6 ? 80 : 64;
   if (S == 5 || S == 6) {
-    const int cands[3] = {96, 80, 64};
+    const int cands[4] = {96, 80, 64, 48};
     long best = -1;
     for (int bn : cands) {
-      if (S == 6 && bn == 96) continue;
+      if (S == 6 && (bn == 96 || bn == 48)) continue;
       const long pad = ((2L * d.N + bn - 1) / bn) * bn;
       if (best < 0 || pad < best) {
         best = pad;
@@ -953,6 +952,9 @@ Geometry geometry(const ZgemmDesc& d, int S, int force_bn = 0) {
   g.kp = ((2 * g.Ktot + KB - 1) / KB) * KB;
   g.rows_a_pad = ((d.M + BM - 1) / BM) * BM;
   if (force_bn) g.BN = force_bn;
+  // two accumulator sets when they fit TMEM: the next tile's MMAs then run while the epilogue
+  // drains the previous tile (S <= 2, or 48-wide tiles at 5 slices)
+  g.nbuf = 2 * S * g.BN <= 512 ? 2 : 1;
   g.rows_b_pad = ((2 * d.N + g.BN - 1) / g.BN) * g.BN;  // B' rows (2 per complex column), whole tiles
   g.ncol_pad = g.rows_b_pad / 2;                        // complex columns incl. padding
   g.rows_b_plane = g.rows_b_pad;
@@ -1057,6 +1059,7 @@ int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const
     case 5096: launch_i8<5, 96>(ta, tb, a, grid, smem, st); break;
     case 5080: launch_i8<5, 80>(ta, tb, a, grid, smem, st); break;
     case 5064: launch_i8<5, 64>(ta, tb, a, grid, smem, st); break;
+    case 5048: launch_i8<5, 48>(ta, tb, a, grid, smem, st); break;
     case 6080: launch_i8<6, 80>(ta, tb, a, grid, smem, st); break;
     case 6064: launch_i8<6, 64>(ta, tb, a, grid, smem, st); break;
     case 7064: launch_i8<7, 64>(ta, tb, a, grid, smem, st); break;

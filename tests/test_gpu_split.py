@@ -106,3 +106,18 @@ def test_autotuner_picks_a_configuration_per_shape_and_keeps_results():
     assert np.array_equal(g1, first) and np.array_equal(g2, first)
     plain.close()
     c.close()
+
+
+@pytest.mark.parametrize("M,N,K", [(300, 24, 500), (130, 72, 52), (1000, 24, 3000)])
+def test_split_zgemm_double_buffered_narrow_tiles(ctx, M, N, K):
+    # 2N a multiple of 48 and of no wider tile: the 5-slice engine runs 48-wide tiles with two
+    # accumulator sets in TMEM (the next tile's MMAs overlap the previous tile's drain)
+    rng = np.random.default_rng(M + N + K)
+    A = rng.standard_normal((M, K)) + 1j * rng.standard_normal((M, K))
+    B = rng.standard_normal((K, N)) + 1j * rng.standard_normal((K, N))
+    A *= np.exp(-0.05 * np.arange(M) / 10)[:, None]
+    ref = A @ B
+    ctx.set_split_slices(5)
+    out = ctx.zgemm(A, B, precision=native.PREC_SPLIT)
+    err = np.abs(out - ref).max(axis=1) / np.abs(ref).max(axis=1)
+    assert err.max() < bound(5, K), err.max()
