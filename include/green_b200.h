@@ -264,8 +264,9 @@ int gg_estimate_bytes(const gg_shape* shape, int64_t num_kpair_stored, int64_t* 
 /* Tile autotuner of the split-precision INT8 engine (no counterpart in the reference, whose
  * GEMMs are cuBLAS calls).  With it enabled, the first call of every distinct GEMM shape on this
  * context that overwrites its output (beta = 0) and is not being captured into a CUDA graph is
- * run once for every candidate tile width (96 / 80 / 64 B' rows at 5 slices) and split-K factor
- * (the wave-filling rule's, one, twice the rule's), timed with CUDA events on the call's stream;
+ * run for every candidate tile width (96 / 80 / 64 / 48 B' rows at 5 slices) and split-K factor
+ * (the wave-filling rule's, one, twice the rule's) - once untimed, once timed with CUDA events on
+ * the call's stream;
  * that call's result and every later call of the shape use the fastest.  Tile width does not
  * change any element's arithmetic; split-K changes only the FP64 summation order of the partial
  * sums.  gg_autotune_report returns one line per tuned shape (valid until the next call on the
