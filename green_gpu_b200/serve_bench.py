@@ -66,8 +66,9 @@ def main(argv=None):
         return jobs
 
     def stream(slots):
+        jobs = jobs_()  # before the server starts, so that its log times start at the stream
         srv = serve.Server(slots=slots)
-        futs = serve.poisson_stream(srv, jobs_(), a.rate, seed=a.seed)
+        futs = serve.poisson_stream(srv, jobs, a.rate, seed=a.seed)
         results = [f.result() for f in futs]
         srv.close()
         return srv, results
