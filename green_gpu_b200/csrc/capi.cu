@@ -610,6 +610,13 @@ int gg_symmetry_unfold(gg_context* c, const double* X_ibz, int64_t nmat, double*
   });
 }
 
+int gg_set_fused_tail(gg_context* c, int enable) {
+  return guarded(c, [&] {
+    c->fused_tail = enable != 0;
+    c->drop_graph();
+  });
+}
+
 int gg_set_autotune(gg_context* c, int enable) {
   return guarded(c, [&] {
     split_set_autotune(split_engine(c), enable != 0);

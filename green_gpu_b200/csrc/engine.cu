@@ -20,6 +20,7 @@
 #include <cstring>
 
 #include "kernels.cuh"
+#include "sigma_tail.cuh"
 #include "split.cuh"
 #include "zgemm.cuh"
 
@@ -626,6 +627,11 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
                                 (size_t)T * NN * sizeof(double2), cudaMemcpyDeviceToHost, st));
     // ---------------- Sigma contributions of the chunk's q stars
     h = tm.begin(6);
+    // the fused tail needs n <= 52 (five n x n blocks in shared memory); larger orbital counts
+    // run X G and Z V^+ as two GEMMs.  Flops of the pair (8MNK + 12MN per complex GEMM).
+    const bool fused_tail = c->fused_tail && sigma_tail_supported(n, T, (long)c->gemm_work.n);
+    const double tail_flops = (double)T * (8.0 * N * n * (double)nn + 12.0 * N * (double)nn) +
+                              8.0 * T * n * (double)n * N * n + 12.0 * T * (double)nn;
     for (int qi = 0; qi < qn; ++qi) {
       const int iq = myq[q0 + qi];
       for (int qd : c->q_stars[iq]) {
@@ -664,15 +670,37 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
             gemm_main(d, 1);
           }
           for (int sp = 0; sp < ns; ++sp) {
+            const double2* Gk = Gf + ((long)k1 * ns + sp) * T * nn;
+            double2* Ck = Sigma_dev + ((long)sp * s.ink + kr) * nn;
+            if (fused_tail) {
+              // Z = X G and Sigma += -1/nk Z V^+ in one kernel (Z stays in registers); FP64 in
+              // both precisions, three-product form inside split builds
+              cudaEvent_t e0 = nullptr, e1 = nullptr;
+              if (c->profiling) {
+                GG_CUDA(cudaEventCreate(&e0));
+                GG_CUDA(cudaEventCreate(&e1));
+                GG_CUDA(cudaEventRecord(e0, st));
+              }
+              c->launches += sigma_tail(SA, Nnn, Gk, Vb, n, N, T, Ck, (long)ns * s.ink * nn,
+                                        make_double2(-1.0 / nk, 0.0), split != nullptr, gw_work,
+                                        (long)c->gemm_work.n, st);
+              c->kstat_flops[2] += tail_flops;
+              c->kstat_launches[2] += 1;
+              if (c->profiling) {
+                GG_CUDA(cudaEventRecord(e1, st));
+                kev.push_back({2, {e0, e1}});
+              }
+              continue;
+            }
             // Z[t][Q][j][c] = sum_l X[t][Q][j][l] G^{k1}(tau_t)[l][c]
             {
               ZgemmDesc d;
               d.M = N * n; d.N = n; d.K = n;
               d.A = SA; d.a_m.lo = n; d.a_k = 1;
-              d.B = Gf + ((long)k1 * ns + sp) * T * nn; d.b_k = n; d.b_n.lo = 1;
+              d.B = Gk; d.b_k = n; d.b_n.lo = 1;
               d.C = SB; d.c_m.lo = n; d.c_n.lo = 1;
               d.nb0 = T; d.a_b0 = Nnn; d.b_b0 = nn; d.c_b0 = Nnn;
-              gemm(d);
+              gemm_main(d, 2, false);
             }
             // Sigma[t][sp][kr][j][i] += -1/nk sum_Q sum_c Z[t][Q][j][c] conj(V[Q][i][c])
             // (one GEMM over all tau: rows m = (t, j), V is the shared operand).  FP64 in both
@@ -683,7 +711,7 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
               d.M = T * n; d.N = n; d.K = n; d.KB = N;
               d.A = SB; d.a_m.split = n; d.a_m.hi = Nnn; d.a_m.lo = n; d.a_k = 1; d.a_kb = nn;
               d.B = Vb; d.b_k = 1; d.b_n.lo = n; d.b_kb = nn; d.conjB = 1;
-              d.C = Sigma_dev + ((long)sp * s.ink + kr) * nn;
+              d.C = Ck;
               d.c_m.split = n; d.c_m.hi = (long)ns * s.ink * nn; d.c_m.lo = n; d.c_n.lo = 1;
               d.alpha = make_double2(-1.0 / nk, 0.0);
               d.beta = make_double2(1.0, 0.0);

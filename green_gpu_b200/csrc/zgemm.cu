@@ -10,6 +10,8 @@
 // copies and the fragment loads are bank-conflict free without padding.
 #include "zgemm.cuh"
 
+#include "dmma.cuh"
+
 #include <atomic>
 
 #include <algorithm>
@@ -21,27 +23,10 @@ constexpr int BM = 64, BN = 64, BK = 8, NT = 128, STAGES = 3;
 constexpr int TILE = BM * BK;  // complex elements per operand stage
 static_assert(BM == BN, "square tiles assumed by the staging code");
 
-__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(c0), "+d"(c1)
-               : "d"(a), "d"(b));
-}
-
 // swizzled position of tile element (row r, k) in a stage
 template <bool KMAJ>
 __device__ __forceinline__ int sidx(int r, int k) {
   return KMAJ ? r * BK + (k ^ ((r & 1) << 2)) : k * BM + (r ^ ((k & 3) << 1));
-}
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  const int n = valid ? 16 : 0;
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
 // One CTA per (tile, split, batch entry) for reductions of any length.

@@ -36,7 +36,7 @@ EXPORTS = [
     "gg_zgemm_noalloc", "gg_set_hf_precision", "gg_estimate_bytes", "gg_set_x2c", "gg_set_graph",
     "gg_batch_create", "gg_batch_run", "gg_batch_destroy", "gg_q_shard_points", "gg_energy_hf", "gg_energy_gw",
     "gg_energy_gw_device", "gg_chemical_potential", "gg_arm_split_timeout_test", "gg_set_autotune",
-    "gg_autotune_report",
+    "gg_autotune_report", "gg_set_fused_tail",
 ]
 
 
@@ -101,6 +101,7 @@ def load(path: str = LIB_PATH):
         "gg_energy_hf": (C.c_int, [P, D, D, D, D]),
         "gg_arm_split_timeout_test": (C.c_int, [P]),
         "gg_set_autotune": (C.c_int, [P, C.c_int]),
+        "gg_set_fused_tail": (C.c_int, [P, C.c_int]),
         "gg_autotune_report": (C.c_char_p, [P]),
         "gg_energy_gw": (C.c_int, [P, D, D, D, D]),
         "gg_energy_gw_device": (C.c_int, [P, P, P, D, D, P]),
@@ -266,6 +267,9 @@ class Context:
         out = np.empty((nmat, s.nk, s.nao, s.nao), np.complex128)
         self._check(self.lib.gg_symmetry_unfold(self.h, _d(X.view(np.float64)), nmat, _d(out.view(np.float64))))
         return out
+
+    def set_fused_tail(self, enable: bool = True):
+        self._check(self.lib.gg_set_fused_tail(self.h, 1 if enable else 0))
 
     def set_autotune(self, enable: bool = True):
         self._check(self.lib.gg_set_autotune(self.h, 1 if enable else 0))

@@ -20,11 +20,13 @@ def main(argv=None):
     ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
     ap.add_argument("--slices", type=int, default=5)
     ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--fused-tail", action="store_true", help="Sigma tail as one kernel (gg_set_fused_tail)")
     a = ap.parse_args(argv)
     mesh = tuple(int(x) for x in a.mesh.split(","))
     s = synth.make_system(mesh=mesh, nao=a.nao, NQ=a.NQ, ns=1, seed=3)
     ctx = native.context_for(s)
     ctx.set_split_slices(a.slices)
+    ctx.set_fused_tail(a.fused_tail)
     prec = native.PREC_SPLIT if a.precision == "split" else native.PREC_FP64
     for _ in range(a.repeat):
         out = ctx.gw_sigma(s.G_tskij, precision=prec)

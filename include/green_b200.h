@@ -125,6 +125,16 @@ int gg_q_shard_points(int32_t inq, int rank, int size, int32_t* q_out, int32_t c
  * 5e-8). */
 int gg_set_split_slices(gg_context* ctx, int slices);
 
+/* Form of the last two steps of the Sigma contraction, Z = X G and the reduction of Z V^+
+ * over (Q, orbital): enable = 1 runs them as one FP64 tensor-core kernel that keeps Z in
+ * registers, for nao <= 52 (larger orbital counts use the two GEMMs); enable = 0 (default) runs
+ * the two GEMMs, with Z in device memory, as src/cugw_qkpt.cu:295-332 does.  The fused form
+ * saves Z's write and read (2 x nts x NQ x nao^2 x 16 bytes per (k, q) pair), but both forms
+ * are bound by the DMMA issue rate, and at nao 52, NQ 400 the fused kernel takes 2.64 ms per
+ * pair against 2.54 ms for the two GEMMs.  Both sum in a fixed order (deterministic); they
+ * differ in the FP64 summation order only. */
+int gg_set_fused_tail(gg_context* ctx, int enable);
+
 /* One GW self-energy build.  G_tskij complex [nts][ns][ink][nao][nao] (host), Sigma_tskij
  * the same shape (host, overwritten: zeroed, accumulated, divided by nk as
  * gw_gpu_kernel::solve does).  solver: GG_SOLVER_*; precision: GG_PREC_*. */
@@ -195,7 +205,8 @@ int gg_last_timings(const gg_context* ctx, double* out, int n);
 /* Per-kernel device time of the last GW build, from CUDA events recorded around every
  * launch of the named contraction on its stream when profiling is enabled:
  * which = 0: the P0 contraction (sum over k of A_k B_k^T), 1: the Sigma contraction
- * (V times W~), 2: the final Sigma product with V^+ (reduction over Q and an orbital).
+ * (V times W~), 2: the Sigma tail, X G and the product with V^+ (reduction over Q and an
+ * orbital), fused or as two GEMMs (gg_set_fused_tail).
  * Writes launches, total seconds and algorithmic flops
  * (8MNK + 12MN per complex GEMM, src/green/gpu/common_defs.h:121-125). */
 int gg_set_profiling(gg_context* ctx, int enable);
