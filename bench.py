@@ -371,13 +371,13 @@ def main():
     achieved = fl / sec / 1e12 if sec > 0 else 0.0
     # the dominant kernels run inside a build of tens of seconds: sustained peaks
     fp64_peak = float(os.environ.get("GG_FP64_PEAK_TFLOPS", "37.0"))
-    kname = ("p0_contraction", "sigma_contraction", "sigma_tail")[dom]
+    kname = ("p0_contraction", "sigma_contraction", "sigma_final_contraction")[dom]
     if args.precision == "fp64" or dom == 2:
-        # the Sigma tail (X G, Z V^+) is FP64 in both precisions
+        # the final product with V^+ is FP64 in both precisions
         peak, peak_note = fp64_peak, ("FP64 tensor (DMMA) rate measured on this pool's B200 with a register-only "
                                       "mma.sync f64 loop (37 TF/s; not part of MEASURED_PEAKS.json)")
         unit = "TFLOP/s"
-        kname += " (X G and Z V^+, FP64 DMMA)" if dom == 2 else " (FP64 DMMA zgemm)"
+        kname += " (FP64 DMMA zgemm)"
     else:
         # executed INT8 work: S(S+1)/2 slice pairs, each a real GEMM of 8MNK ops per complex GEMM
         pairs = args.slices * (args.slices + 1) // 2

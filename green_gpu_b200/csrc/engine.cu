@@ -700,7 +700,7 @@ void gw_build(gg_context* c, const double2* G_dev, double2* Sigma_dev, int solve
               d.B = Gk; d.b_k = n; d.b_n.lo = 1;
               d.C = SB; d.c_m.lo = n; d.c_n.lo = 1;
               d.nb0 = T; d.a_b0 = Nnn; d.b_b0 = nn; d.c_b0 = Nnn;
-              gemm_main(d, 2, false);
+              gemm(d);
             }
             // Sigma[t][sp][kr][j][i] += -1/nk sum_Q sum_c Z[t][Q][j][c] conj(V[Q][i][c])
             // (one GEMM over all tau: rows m = (t, j), V is the shared operand).  FP64 in both

@@ -225,8 +225,48 @@ __device__ __forceinline__ void drain_cols(uint32_t taddr, double* acc, double s
   }
 }
 
+// drain two adjacent diagonals d, d + 1 (`NC` int32 columns each, a multiple of 4, at most 16,
+// starting at ta and tb) as one value 128 acc_d + acc_{d+1} = 2^7(d+1) (acc_d 2^-7d +
+// acc_{d+1} 2^-7(d+1)): one conversion and one FMA per column pair instead of two each.  Exact
+// when |128 acc_d| + |acc_{d+1}| < 2^31, which the host checks for the K segments of the launch
+// (I8Args::pair).
+template <int NC>
+__device__ __forceinline__ void drain_pair_cols(uint32_t ta, uint32_t tb, double* acc, double scale) {
+  static_assert(NC % 4 == 0 && NC <= 16, "TMEM loads of 4, 8 or 16 columns");
+  int r[16], q[16];
+  if constexpr (NC == 16) {
+    tmem_ld16(ta, r);
+    tmem_ld16(tb, q);
+  } else {
+    if constexpr (NC >= 8) {
+      tmem_ld8(ta, r);
+      tmem_ld8(tb, q);
+    }
+    if constexpr (NC % 8 == 4) {
+      tmem_ld4(ta + (NC / 8) * 8, r + (NC / 8) * 8);
+      tmem_ld4(tb + (NC / 8) * 8, q + (NC / 8) * 8);
+    }
+  }
+  tmem_wait_ld();
+#pragma unroll
+  for (int j = 0; j < NC / 4; ++j) {
+    reg_fence4(r + j * 4);
+    reg_fence4(q + j * 4);
+  }
+#pragma unroll
+  for (int i = 0; i < NC; ++i) {
+    const int v = r[i] * 128 + q[i];
+    const double x = __hiloint2double(0x43380000, v ^ (int)0x80000000) - 6755401588539392.0;
+    acc[i] = fma(x, scale, acc[i]);
+  }
+}
+
+// biased exponent of |x| (0 for x = 0); every nonzero accumulator value is a normal number
+__device__ __forceinline__ int biased_exponent(double x) { return (__double2hiint(x) >> 20) & 0x7ff; }
+
 struct I8Args {
   int S;
+  int pair;  // the epilogue drains diagonals (2, 3), (4, 5), ... as pairs (exact: see drain_pair_cols)
   int rows_a_pad, rows_b_pad;  // per (batch, slice)
   int nkb;                     // K blocks of 64 bytes
   int kcb;                     // K blocks per exact int32 chunk
@@ -500,20 +540,36 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         // unrolled form made the epilogue larger than the instruction cache, which stalled
         // the short-K GEMMs whose epilogue runs after every two K blocks)
 #pragma unroll 1
-        for (int d = 2; d <= S + 1; ++d) {
+        for (int d = 2; d <= S + 1;) {
+          const bool two = p.pair && d + 1 <= S + 1;
           if (!mbar_wait(&accf[buf * ND + d - 2], par, err, 8, p.wait_cycles)) { ok = false; break; }
+          if (two && !mbar_wait(&accf[buf * ND + d - 1], par, err, 8, p.wait_cycles)) { ok = false; break; }
           tc_fence_after();
-          const double scale = __longlong_as_double((long long)(1023 - 7 * d) << 52);  // 2^-7d
+          const int dl = two ? d + 1 : d;
+          const double scale = __longlong_as_double((long long)(1023 - 7 * dl) << 52);  // 2^-7dl
           const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)buf * buf_cols +
                                 (uint32_t)((d - 2) * BN + h * HC);
-          // groups of 32 columns, one wait per group
+          if (two) {
+            // groups of 8 columns of both diagonals, one wait per group (16 loaded registers:
+            // wider groups spill at the register budget of 576 threads)
 #pragma unroll
-          for (int j = 0; j < HC / 32; ++j) drain_cols<32>(base + j * 32, acc + j * 32, scale);
-          if constexpr (HC % 32 != 0) drain_cols<HC % 32>(base + (HC / 32) * 32, acc + (HC / 32) * 32, scale);
+            for (int j = 0; j < HC / 8; ++j) drain_pair_cols<8>(base + j * 8, base + BN + j * 8, acc + j * 8, scale);
+            if constexpr (HC % 8 != 0)
+              drain_pair_cols<HC % 8>(base + (HC / 8) * 8, base + BN + (HC / 8) * 8, acc + (HC / 8) * 8, scale);
+          } else {
+            // groups of 32 columns, one wait per group
+#pragma unroll
+            for (int j = 0; j < HC / 32; ++j) drain_cols<32>(base + j * 32, acc + j * 32, scale);
+            if constexpr (HC % 32 != 0) drain_cols<HC % 32>(base + (HC / 32) * 32, acc + (HC / 32) * 32, scale);
+          }
           tc_fence_before();
           __syncwarp();
           const bool withheld = p.skip_arrive && blockIdx.x == 0 && warp == 2 && u == blockIdx.x && d == 2;
-          if (lane == 0 && !withheld) mbar_arrive(&acce[buf * ND + d - 2]);
+          if (lane == 0) {
+            if (!withheld) mbar_arrive(&acce[buf * ND + d - 2]);
+            if (two) mbar_arrive(&acce[buf * ND + d - 1]);
+          }
+          d += two ? 2 : 1;
         }
         if (++buf == p.nbuf) {
           buf = 0;
@@ -540,25 +596,30 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const int xmq = m / p.mx.div_m, xmr = m - xmq * p.mx.div_m;
         const long xrow = w.batch * p.mx.s_b + xmq * p.mx.s_mq + xmr * p.mx.s_mr;
         int xq = nbase / p.mx.div_n, xr = nbase - xq * p.mx.div_n;
-        double xmax = 0.0;
+        // in exponents: ilogb(|acc| 2^(ea + eb + 2)) = ilogb|acc| + ea + eb + 2, so the largest
+        // exponent of a run is found with integer maxima (the result is that of the largest
+        // scaled value); kNone marks a run without a nonzero value
+        constexpr int kNone = -(1 << 30);
+        const int xoff = ea + 2 - 1023;
+        int xe = kNone;
         auto xflush = [&](int colkey) {
           const long idx = xrow + colkey * p.mx.s_nq;
 #pragma unroll
           for (int off = 1; off < 32; off <<= 1) {
-            const double o = __shfl_down_sync(0xffffffffu, xmax, off);
+            const int o = __shfl_down_sync(0xffffffffu, xe, off);
             const long oi = __shfl_down_sync(0xffffffffu, idx, off);
-            if (lane + off < 32 && oi == idx) xmax = fmax(xmax, o);
+            if (lane + off < 32 && oi == idx) xe = max(xe, o);
           }
           const long prev = __shfl_up_sync(0xffffffffu, idx, 1);
-          if ((lane == 0 || prev != idx) && xmax > 0.0) atomicMax(p.mx.ex + idx, ilogb(xmax) + 1);
-          xmax = 0.0;
+          if ((lane == 0 || prev != idx) && xe != kNone) atomicMax(p.mx.ex + idx, xe + 1);
+          xe = kNone;
         };
 #pragma unroll
         for (int c = 0; c < HC / 2; ++c) {
           const int eb = __shfl_sync(0xffffffffu, eb_lane, c);
           if (mok && nbase + c < p.N) {
-            const double sb = pow2i(eb + 2);
-            xmax = fmax(xmax, fmax(fabs(acc[2 * c] * sa * sb), fabs(acc[2 * c + 1] * sa * sb)));
+            const int be = max(biased_exponent(acc[2 * c]), biased_exponent(acc[2 * c + 1]));
+            if (be != 0) xe = max(xe, be + eb + xoff);
           }
           if (++xr == p.mx.div_n) {
             xflush(xq);
@@ -1051,6 +1112,14 @@ int run_planes(SplitGemm* e, const ZgemmDesc& d, int S, const Geometry& g, const
     e->work.ensure((size_t)splits * need);
   }
   a.splits = splits;
+  // pairs (d, d+1), d = 2, 4, ...: |acc_d| <= (d - 1) Kc 64^2 for a segment of Kc bytes, so the
+  // combined value 128 acc_d + acc_{d+1} stays below 2^31 when (128 (d-1) + d) Kc 4096 < 2^31
+  // for the largest paired d (the even d <= S)
+  {
+    const long seg = std::min<long>(g.kcb, (g.nkb + splits - 1) / splits) * KB;
+    const long dmax = (S / 2) * 2;
+    a.pair = (128 * (dmax - 1) + dmax) * seg * 4096L < (1L << 31) ? 1 : 0;
+  }
   a.work = e->work.p;
   a.units = base * splits;
   if (a.units >= (1L << 31) || (long)splits * g.nkb >= (1L << 31))

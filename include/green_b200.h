@@ -205,8 +205,9 @@ int gg_last_timings(const gg_context* ctx, double* out, int n);
 /* Per-kernel device time of the last GW build, from CUDA events recorded around every
  * launch of the named contraction on its stream when profiling is enabled:
  * which = 0: the P0 contraction (sum over k of A_k B_k^T), 1: the Sigma contraction
- * (V times W~), 2: the Sigma tail, X G and the product with V^+ (reduction over Q and an
- * orbital), fused or as two GEMMs (gg_set_fused_tail).
+ * (V times W~), 2: the final Sigma product with V^+ (reduction over Q and an orbital), or with
+ * gg_set_fused_tail the fused kernel that also forms its operand Z = X G.  Each entry covers
+ * launches of one kernel kind.
  * Writes launches, total seconds and algorithmic flops
  * (8MNK + 12MN per complex GEMM, src/green/gpu/common_defs.h:121-125). */
 int gg_set_profiling(gg_context* ctx, int enable);
