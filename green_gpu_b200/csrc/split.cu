@@ -202,9 +202,6 @@ __device__ __forceinline__ double pow2i(int e) {
   return __longlong_as_double((long long)(e + 1023) << 52);
 }
 
-// 2^e for e in the normal range (exact)
-__device__ __forceinline__ double scale_pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
-
 // drain `NC` int32 columns (a multiple of 4, at most 32) starting at taddr into acc * scale
 template <int NC>
 __device__ __forceinline__ void drain_cols(uint32_t taddr, double* acc, double scale) {
