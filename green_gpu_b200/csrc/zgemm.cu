@@ -23,6 +23,11 @@ constexpr int BM = 64, BN = 64, BK = 8, NT = 128, STAGES = 3;
 constexpr int TILE = BM * BK;  // complex elements per operand stage
 static_assert(BM == BN, "square tiles assumed by the staging code");
 
+// x with its sign bit XORed with the sign bit of `s` (s = 0 or 0x80000000)
+__device__ __forceinline__ double flip(double x, int s) {
+  return __hiloint2double(__double2hiint(x) ^ s, __double2loint(x));
+}
+
 // swizzled position of tile element (row r, k) in a stage
 template <bool KMAJ>
 __device__ __forceinline__ int sidx(int r, int k) {
@@ -118,8 +123,9 @@ __global__ void __launch_bounds__(NT, 2)
   };
   zero_acc();
 
-  const double sa = d.conjA ? -1.0 : 1.0;
-  const double sb = d.conjB ? -1.0 : 1.0;
+  // conjugation flips the sign bit of the imaginary part (an integer XOR, no FP64 multiply)
+  const int sa = d.conjA ? (int)0x80000000 : 0;
+  const int sb = d.conjB ? (int)0x80000000 : 0;
   const int fr = lane >> 2, fk = lane & 3;
 
   auto epilogue = [&](int m0, int n0) {
@@ -178,14 +184,14 @@ __global__ void __launch_bounds__(NT, 2)
         for (int mt = 0; mt < 4; ++mt) {
           const double2 v = as[sidx<A_K>(wm * 32 + mt * 8 + fr, ks * 4 + fk)];
           ar[mt] = v.x;
-          ai[mt] = sa * v.y;
+          ai[mt] = flip(v.y, sa);
           an[mt] = -ai[mt];
         }
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
           const double2 v = bs[sidx<B_K>(wn * 32 + nt * 8 + fr, ks * 4 + fk)];
           br[nt] = v.x;
-          bi[nt] = sb * v.y;
+          bi[nt] = flip(v.y, sb);
         }
 #pragma unroll
         // four passes over the 16 accumulator tiles: consecutive DMMAs never share an
@@ -349,8 +355,9 @@ __global__ void __launch_bounds__(NT8, 2)
   };
   zero_acc();
 
-  const double sa = d.conjA ? -1.0 : 1.0;
-  const double sb = d.conjB ? -1.0 : 1.0;
+  // conjugation flips the sign bit of the imaginary part (an integer XOR, no FP64 multiply)
+  const int sa = d.conjA ? (int)0x80000000 : 0;
+  const int sb = d.conjB ? (int)0x80000000 : 0;
   const int fr = lane >> 2, fk = lane & 3;
 
   auto epilogue = [&](int m0, int n0) {
@@ -390,14 +397,14 @@ __global__ void __launch_bounds__(NT8, 2)
     for (int mt = 0; mt < FM8; ++mt) {
       const double2 v = as[sidx<A_K>(wm * WM8 + mt * 8 + fr, ks * 4 + fk)];
       ar[mt] = v.x;
-      ai[mt] = sa * v.y;
+      ai[mt] = flip(v.y, sa);
       ax[mt] = G3 ? ar[mt] + ai[mt] : -ai[mt];
     }
 #pragma unroll
     for (int nt = 0; nt < FN8; ++nt) {
       const double2 v = bs[sidx<B_K>(wn * WN8 + nt * 8 + fr, ks * 4 + fk)];
       br[nt] = v.x;
-      bi[nt] = sb * v.y;
+      bi[nt] = flip(v.y, sb);
       bx[nt] = br[nt] + bi[nt];
     }
     if constexpr (G3) {
