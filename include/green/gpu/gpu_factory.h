@@ -9,6 +9,7 @@
 #ifndef GREEN_GPU_FACTORY_H
 #define GREEN_GPU_FACTORY_H
 
+#include <Eigen/Dense>
 #include <hdf5.h>
 #include <hdf5_hl.h>
 
@@ -152,9 +153,9 @@ namespace green::gpu {
   class scalar_gw_gpu_kernel {
   public:
     // x2c = true is x2c_gw_gpu_kernel (gw_gpu_kernel.h:131-206): nso = 2 nao, ns = 1
-    scalar_gw_gpu_kernel(const params::params& p, size_t nao, size_t nso, size_t ns, size_t NQ,
-                         const grids::transformer_t& ft, const bz_utils_t& bz, LinearSolverType solver, int verbose = 1,
-                         bool x2c = false) :
+    scalar_gw_gpu_kernel(const params::params& p, size_t nao, [[maybe_unused]] size_t nso, size_t ns, size_t NQ,
+                         const grids::transformer_t& ft, const bz_utils_t& bz, LinearSolverType solver,
+                         [[maybe_unused]] int verbose = 1, bool x2c = false) :
         _ctx(detail::shape(bz, nao, NQ, ns, ft.sd().repn_fermi().nts(), ft.sd().repn_bose().nw())),
         _solver(solver == LinearSolverType::Cholesky ? GG_SOLVER_CHOLESKY : GG_SOLVER_LU),
         _precision((p["P_sp"].as<bool>() && p["Sigma_sp"].as<bool>()) ? GG_PREC_SPLIT : GG_PREC_FP64) {
@@ -190,7 +191,7 @@ namespace green::gpu {
 
   inline std::tuple<std::shared_ptr<void>, std::function<void(G_type&, G_type&)>> custom_gw_kernel(
       bool X2C, const params::params& p, size_t nao, size_t nso, size_t ns, size_t NQ, const grids::transformer_t& ft,
-      const bz_utils_t& bz_utils, const ztensor<4>& S_k) {
+      const bz_utils_t& bz_utils, [[maybe_unused]] const ztensor<4>& S_k) {
     std::shared_ptr<void> kernel(
         new scalar_gw_gpu_kernel(p, nao, nso, ns, NQ, ft, bz_utils, p["cuda_linear_solver"], p["verbose"], X2C));
     std::function<void(G_type&, G_type&)> callback = [kernel](G_type& g, G_type& s) {

@@ -50,3 +50,14 @@ def test_cpp_wrapper_runs_gw_and_hf(tmp_path):
     assert np.abs(Sigma - ref).max() < 1e-10 * np.abs(ref).max()
     kref = ohf.exchange(s, s.dm)
     assert np.abs(K - kref).max() < 1e-10 * np.abs(kref).max()
+
+
+def test_drop_in_header_compiles():
+    # the green-mbpt drop-in (include/green/gpu/gpu_factory.h) against stand-ins of the green-*,
+    # HDF5 and Eigen headers that declare what green-gpu's plugin code uses of them: every call
+    # from the drop-in into the C++ wrapper is type-checked
+    src = os.path.join(ROOT, "tests", "cpp", "drop_in_compile.cpp")
+    cmd = ["g++", "-std=c++17", "-fsyntax-only", "-Wall", "-Wextra", "-Werror", "-I",
+           os.path.join(ROOT, "tests", "cpp", "stubs"), "-I", os.path.join(ROOT, "include"), src]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
