@@ -8,6 +8,7 @@ multiples of 4 or 8, the largest fused count (52) and one above it (the two-GEMM
 import numpy as np
 import pytest
 
+import fixture
 from green_gpu_b200 import native, synth
 from oracle import gw as ogw
 
@@ -78,3 +79,23 @@ def test_tail_kernel_statistics():
     assert stats[False]["flops"] == pytest.approx(stats[False]["launches"] * zv, rel=1e-12)
     assert stats[True]["flops"] == pytest.approx(stats[True]["launches"] * (xg + zv), rel=1e-12)
     assert stats[True]["seconds"] > 0 and stats[False]["seconds"] > 0
+
+
+@pytest.mark.parametrize("precision", [native.PREC_FP64, native.PREC_SPLIT])
+def test_fused_tail_with_space_group_symmetry(precision):
+    # the reference's 27 -> 4 k fixture: rotated W~ (U_q) and k-pair conj/trans lists feed the tail
+    s, _ = fixture.load(gw=True)
+    nts, nw = s.nts, 41
+    rng = np.random.default_rng(11)
+    s.nw_b = nw
+    s.Ttn_FB = 0.05 * (rng.standard_normal((nts, nw)) + 1j * rng.standard_normal((nts, nw)))
+    s.Tnt_BF = 0.05 * (rng.standard_normal((nw, nts - 2)) + 1j * rng.standard_normal((nw, nts - 2)))
+    ctx = native.context_for(s)
+    try:
+        ctx.set_fused_tail(False)
+        two = ctx.gw_sigma(s.G_tskij, solver=native.SOLVER_LU, precision=precision)
+        ctx.set_fused_tail(True)
+        fused = ctx.gw_sigma(s.G_tskij, solver=native.SOLVER_LU, precision=precision)
+    finally:
+        ctx.close()
+    assert rel(fused, two) < TOL_FORMS
